@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Throughput of the B200 optical-photon transport.
+
+Workload (one "step" = one pass over it):
+  scan256  (default) BGO + ESR crystal 48x48x22.4 mm, 256 emission points
+           uniform in the volume (Philox key 7), 200,000 isotropic photons per
+           point = 51.2M photons, per-point 8x8 count and first-hit maps.
+  point1m  CsI(Tl) + Teflon 48x48x37.2 mm, 1,000,000 photons from the centre,
+           8x8x81 count histogram and 8x8 first-hit map.
+
+Arms:
+  --impl cuda       (default) the sm_100a library; `value` = photons/s with
+                    inputs resident in HBM (device entry point, CUDA events on
+                    the launch stream, L2 flushed between steps); `e2e` =
+                    photons/s through the host-buffer C-ABI call (pinned host
+                    inputs copied in, maps/times/counters copied out).
+  --impl reference  the CPU restatement of the reference's transport
+                    (oracle/, all host threads) on a bounded sample of the
+                    same workload; the reference itself is Julia, absent here.
+
+Multi-GPU (torchrun): every rank transports its own full workload with a
+disjoint photon-id range (weak scaling, no data-path collective); the time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np
+
+# Reference operations per photon-step (Float32/int arithmetic of the reference's
+# transport expressions, log/sin/cos/sqrt/div one each), counted by the
+# instrumented oracle (python -m oracle.opcount).
+OPS_PER_STEP = {"scan256": 165.6, "point1m": 186.7}
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload(name: str):
+    from crysplight_b200.params import (Box, OpticalParams, Readout, SipmGrid, TimeBinning,
+                                        deg2rad_f32)
+    from crysplight_b200.scan import scan_points
+    grid, tb = SipmGrid(6.0, 8, 8), TimeBinning(100.0, 80)
+    if name == "scan256":
+        box = Box((48.0, 48.0, 22.4))
+        op = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, deg2rad_f32(1.3), 1.0)
+        pts = scan_points(256, box, seed=7)
+        return dict(name=name, box=box, op=op, ro=Readout(grid), tb=tb, tau=1768.0, seed=1234,
+                    points=pts, per_point=200_000, n=256 * 200_000,
+                    desc="BGO+ESR 48x48x22.4 mm, 256 points x 200000 photons, per-point 8x8 maps")
+    box = Box((48.0, 48.0, 37.2))
+    op = OpticalParams(1.79, 1.45, 3115.0, 346.0, 0.99, False, True, deg2rad_f32(1.3), 1.0)
+    return dict(name=name, box=box, op=op, ro=Readout(grid), tb=tb, tau=1000.0, seed=1234,
+                points=np.float32([[24.0, 24.0, 18.6]]), per_point=1_000_000, n=1_000_000,
+                desc="CsI(Tl)+Teflon 48x48x37.2 mm, 1e6 photons from the centre, 8x8x81 histogram")
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"cl_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        busy = [v for v in sm if smax and v > 0.3 * smax] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "fallback": True}
+
+
+# ------------------------------------------------------------------------------------
+# reference arm / CPU baseline: the oracle on the host cores
+# ------------------------------------------------------------------------------------
+def cpu_run(W, n_points: int, per_point: int) -> tuple[float, int]:
+    from oracle import oracle
+    pts = W["points"][:n_points]
+    t0 = time.perf_counter()
+    if W["name"] == "scan256":
+        oracle.run_segments(W["box"], W["op"], W["ro"], W["tb"], sources=pts,
+                            photons_per_source=[per_point] * n_points,
+                            segment_of_source=range(n_points), n_segments=n_points,
+                            seed=W["seed"], tau_ns=W["tau"], nthreads=os.cpu_count())
+    else:
+        oracle.run_photons(W["box"], W["op"], W["ro"], W["tb"], n_photons=per_point,
+                           seed=W["seed"], pos=tuple(pts[0]), tau_ns=W["tau"],
+                           nthreads=os.cpu_count())
+    dt = time.perf_counter() - t0
+    return dt, n_points * per_point
+
+
+def cpu_sample_size(W, target_s: float) -> tuple[int, int]:
+    """(points, photons per point) of a sample that takes about target_s."""
+    if W["name"] == "scan256":
+        dt, n = cpu_run(W, 1, 20_000)
+        pts = int(max(1, min(256, target_s / (dt * W["per_point"] / 20_000))))
+        return pts, W["per_point"]
+    dt, n = cpu_run(W, 1, 50_000)
+    per = int(max(50_000, min(W["per_point"] * 50, target_s / dt * 50_000)))
+    return 1, per
+
+
+def cpu_baseline(W, target_s: float) -> dict:
+    pts, per = cpu_sample_size(W, target_s)
+    dt, n = cpu_run(W, pts, per)
+    return {"value": n / dt, "unit": "photons/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{pts} point(s) x {per} photons of the {W['name']} workload "
+                      f"({dt:.1f} s on {os.cpu_count()} threads)"}
+
+
+def run_reference_arm(args, W, rank, world):
+    if rank != 0:
+        return
+    pts, per = cpu_sample_size(W, args.cpu_seconds)
+    for _ in range(args.warmup):
+        cpu_run(W, pts, per)
+    times = []
+    for _ in range(args.steps):
+        dt, n = cpu_run(W, pts, per)
+        times.append(dt)
+    tot_n = n * args.steps
+    value = tot_n / sum(times)
+    sample = (f"{pts} point(s) x {per} photons of the {W['name']} workload per step "
+              f"(C restatement of the reference CPU transport, {os.cpu_count()} threads)")
+    line = {
+        "impl": "reference", "metric": "photons/s", "value": value, "unit": "photons/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": W["name"], "desc": W["desc"], "sample_photons_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "photons/s", "cores": os.cpu_count(),
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------
+# CUDA arm
+# ------------------------------------------------------------------------------------
+def run_cuda_arm(args, W, rank, world, local_rank):
+    import torch
+    import crysplight_b200 as cl
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    eng = cl.Engine(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    pid_base = rank * W["n"]        # disjoint photon ids per rank
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+    nx = ny = 8
+    pts = W["points"]
+    npts = pts.shape[0]
+    if W["name"] == "scan256":
+        off = np.zeros(npts + 1, np.int64)
+        off[1:] = np.cumsum(np.full(npts, W["per_point"], np.int64))
+        seg = np.arange(npts, dtype=np.int32)
+        d_sx = torch.from_numpy(np.ascontiguousarray(pts[:, 0])).to(dev)
+        d_sy = torch.from_numpy(np.ascontiguousarray(pts[:, 1])).to(dev)
+        d_sz = torch.from_numpy(np.ascontiguousarray(pts[:, 2])).to(dev)
+        d_off = torch.from_numpy(off).to(dev)
+        d_seg = torch.from_numpy(seg).to(dev)
+        d_maps = torch.empty(nx * ny * npts, dtype=torch.int32, device=dev)
+        d_tmin = torch.empty(nx * ny * npts, dtype=torch.float32, device=dev)
+        d_npe = torch.empty(npts, dtype=torch.int32, device=dev)
+        d_ctr = torch.empty(9, dtype=torch.int64, device=dev)
+
+        def device_step():
+            eng.run_segments_device(
+                W["box"], W["op"], W["ro"], W["tb"], sx=d_sx.data_ptr(), sy=d_sy.data_ptr(),
+                sz=d_sz.data_ptr(), st=None, src_offsets=d_off.data_ptr(),
+                src_segment=d_seg.data_ptr(), n_src=npts, n_segments=npts, n_photons=W["n"],
+                seed=W["seed"], pid_offset=pid_base, tau_ns=W["tau"], maps=d_maps.data_ptr(),
+                tmin=d_tmin.data_ptr(), npe=d_npe.data_ptr(), counters=d_ctr.data_ptr(),
+                stream=sptr)
+
+        # pinned host inputs for the end-to-end path
+        h_pts = torch.from_numpy(np.ascontiguousarray(pts)).pin_memory().numpy()
+        h_cnt = torch.full((npts,), W["per_point"], dtype=torch.int64).pin_memory().numpy()
+        h_seg = torch.from_numpy(seg).pin_memory().numpy()
+
+        def host_step():
+            return eng.run_segments(W["box"], W["op"], W["ro"], W["tb"], sources=h_pts,
+                                    photons_per_source=h_cnt, segment_of_source=h_seg,
+                                    n_segments=npts, seed=W["seed"], pid_offset=pid_base,
+                                    tau_ns=W["tau"])
+        h2d = 3 * 4 * npts + 8 * (npts + 1) + 4 * npts
+        d2h = 2 * 4 * nx * ny * npts + 4 * npts + 72 + 12
+        out_bytes = 2 * 4 * nx * ny * npts + 4 * npts + 72
+        launches = 3
+    else:
+        d_p = [torch.from_numpy(np.ascontiguousarray(pts[:, i])).to(dev) for i in range(3)]
+        nb = W["tb"].nbins + 1
+        d_counts = torch.empty(nx * ny * nb, dtype=torch.int32, device=dev)
+        d_first = torch.empty(nx * ny, dtype=torch.float32, device=dev)
+        d_ctr = torch.empty(9, dtype=torch.int64, device=dev)
+
+        def device_step():
+            eng.run_photons_device(W["box"], W["op"], W["ro"], W["tb"], px=d_p[0].data_ptr(),
+                                   py=d_p[1].data_ptr(), pz=d_p[2].data_ptr(), pt=None, npos=1,
+                                   n_photons=W["n"], seed=W["seed"], pid_offset=pid_base,
+                                   tau_ns=W["tau"], counts=d_counts.data_ptr(),
+                                   first_ns=d_first.data_ptr(), counters=d_ctr.data_ptr(),
+                                   stream=sptr)
+        h_pos = tuple(float(v) for v in pts[0])
+
+        def host_step():
+            return eng.run_photons_ka(W["box"], W["op"], W["ro"], W["tb"], n_photons=W["n"],
+                                      seed=W["seed"], pos=h_pos, pid_offset=pid_base,
+                                      tau_ns=W["tau"])
+        h2d = 3 * 4
+        d2h = 4 * nx * ny * nb + 4 * nx * ny + 72 + 12
+        out_bytes = 4 * nx * ny * nb + 4 * nx * ny + 72
+        launches = 2
+
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # warm-up
+    for _ in range(args.warmup):
+        device_step()
+    eng.sync(sptr)
+    host_step()
+
+    # ---- device-resident timing ----
+    clocks = ClockSampler(local_rank)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    clocks.start()
+    t_wall0 = time.perf_counter()
+    for i in range(args.steps):
+        flush.zero_()                       # evict L2 between timed steps
+        starts[i].record(stream)
+        device_step()
+        stops[i].record(stream)
+    eng.sync(sptr)
+    barrier()
+    t_wall = time.perf_counter() - t_wall0
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    steps_per_launch = eng.last_steps
+    tot_ms = sum(step_ms)
+
+    # ---- end-to-end through the host-buffer C-ABI ----
+    barrier()
+    e2e_t0 = time.perf_counter()
+    for _ in range(args.steps):
+        host_step()
+    barrier()
+    e2e_s = time.perf_counter() - e2e_t0
+
+    if dist is not None:
+        t = torch.tensor([tot_ms, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms, e2e_s = float(t[0]), float(t[1])
+
+    if rank != 0:
+        eng.close()
+        return
+    n_total = W["n"] * args.steps * world
+    value = n_total / (tot_ms * 1e-3)
+    e2e_value = n_total / e2e_s
+    peaks = measured_peaks()
+    props = torch.cuda.get_device_properties(dev)
+    n_sm = props.multi_processor_count
+    launch_s = tot_ms * 1e-3 / args.steps
+    ops_step = OPS_PER_STEP[W["name"]]
+    achieved = ops_step * steps_per_launch / launch_s
+    peak = n_sm * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6
+    line = {
+        "metric": "photons/s", "value": value, "unit": "photons/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": W["name"], "desc": W["desc"], "photons_per_step_per_gpu": W["n"],
+                   "l2": "flushed between timed steps (256 MiB memset)",
+                   "parallelism": f"photon-range shards x{world}"},
+        "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches * args.steps,
+        "photon_steps_per_launch": steps_per_launch,
+        "photon_steps_per_s": steps_per_launch / launch_s,
+        "roofline": {
+            "bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gop/s",
+            "frac": achieved / peak, "traffic": None,
+            "ops_per_step": ops_step,
+            "note": ("reference Float32/int ops per photon-step x steps / launch time, against "
+                     "one op per lane per clock (SMs x 128 lanes x max SM clock of measured)"),
+            "hbm": {"achieved": out_bytes / launch_s / 1e9, "peak": peaks.get("hbm_gbs"),
+                    "unit": "GB/s", "frac": out_bytes / launch_s / 1e9 / peaks.get("hbm_gbs", 1)},
+        },
+        "clocks": clk,
+        "wall_s_timed": t_wall,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(W, args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
+    ap.add_argument("--workload", choices=("scan256", "point1m"), default="scan256")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    W = workload(args.workload)
+    if args.impl == "reference":
+        run_reference_arm(args, W, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_cuda_arm(args, W, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,975 @@
+// cl_transport.cu — sm_100a transport kernels and the C-ABI of
+// include/crysplight_cuda.h.
+//
+// Kernel design (B200):
+//   * persistent grid: (#SM x resident CTAs) CTAs of 256 threads; every warp
+//     claims photon chunks from a device work queue (one 64-bit atomic per
+//     chunk) and each lane refills itself with the next photon the moment
+//     its photon terminates, so long-bouncing photons never idle a warp;
+//   * parameters travel as a __grid_constant__ kernel argument (constant
+//     bank), the log table sits in shared memory;
+//   * point mode: the nx*ny*(nbins+1) count tile and the nx*ny first-time
+//     tile live in shared memory; detections are warp-aggregated with
+//     __match_any_sync (one shared atomic per distinct bin per warp step),
+//     first times use atomicMin on order-preserving uint32 keys; each CTA
+//     flushes its tile once with coalesced global atomics and the last CTA
+//     decodes the first-time keys in place;
+//   * segment mode (scan points, 511 keV events): per-segment 8x8 maps and
+//     first-time keys are reduced with warp-aggregated global atomics;
+//     a finalize kernel decodes keys and sums npe.
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <new>
+
+#include <cuda_runtime.h>
+#include <curand_philox4x32_x.h>
+
+#include "../../include/crysplight_cuda.h"
+#include "cl_device.cuh"
+
+#define CL_VERSION_STRING "crysplight_b200 0.1.0 (sm_100a)"
+
+namespace cl {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int LOGTAB_BYTES = ((CLM_LOG_NTAB * 16 + 127) / 128) * 128;
+
+__constant__ double c_logtab[2 * CLM_LOG_NTAB] = { CLM_LOG_TAB_INIT };
+
+struct KArgs {
+    Physics P;
+    uint64_t pid0;
+    int64_t n;
+    int32_t npos;
+    int32_t warp_chunk;
+    int32_t cells;        // nx*ny
+    int32_t bins_total;   // nbins+1
+    const float* px; const float* py; const float* pz; const float* pt;
+    const int64_t* src_off; const int32_t* src_seg; int64_t n_src;
+    uint32_t* counts;     // point: cells*bins_total
+    uint32_t* keys;       // point: cells; segments: cells*n_seg
+    uint32_t* maps;       // segments: cells*n_seg
+    unsigned long long* counters;  // 9 x int64, cl_counters order
+    uint8_t* r_status; int16_t* r_idx; float* r_t; int32_t* r_bounces;
+    unsigned long long* queue;
+    unsigned long long* steps;
+    unsigned int* done;
+    unsigned int* err;
+};
+
+__device__ __forceinline__ int time_bin0(float t, const Physics& P)
+{
+    // 1 + unsafe_trunc(t / bin_ns), overflow -> nbins+1 (src/transport.jl:100-101), 0-based
+    const float q = t / P.bin_ns;
+    if (!(q < (float)P.nbins)) return P.nbins;
+    const int b = (int)q;
+    return b < 0 ? 0 : b;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// Galloping search: largest s >= hint with off[s] <= k (off[n_src] = total).
+__device__ __forceinline__ int64_t find_source(const int64_t* __restrict__ off, int64_t n_src,
+                                               int64_t hint, int64_t k)
+{
+    int64_t lo = hint, step = 1;
+    int64_t hi = hint + 1;
+    while (hi < n_src && __ldg(off + hi) <= k) {
+        lo = hi;
+        step <<= 1;
+        hi = lo + step;
+    }
+    if (hi > n_src) hi = n_src;
+    // invariant: off[lo] <= k < off[hi]  (off[n_src] > k)
+    while (hi - lo > 1) {
+        const int64_t mid = lo + ((hi - lo) >> 1);
+        if (__ldg(off + mid) <= k) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <int MODE, bool REC, bool TILE>
+__global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ KArgs A)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* s_tab = reinterpret_cast<double2*>(smem);
+    uint32_t* s_counts = reinterpret_cast<uint32_t*>(smem + LOGTAB_BYTES);
+    uint32_t* s_keys = s_counts + (TILE ? A.cells * A.bins_total : 0);
+    __shared__ unsigned long long s_cnt[10];
+    __shared__ unsigned int s_last;
+
+    const Physics& P = A.P;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < CLM_LOG_NTAB; i += blockDim.x)
+        s_tab[i] = make_double2(c_logtab[2 * i], c_logtab[2 * i + 1]);
+    if (TILE) {
+        const int nt = A.cells * A.bins_total;
+        for (int i = tid; i < nt; i += blockDim.x) s_counts[i] = 0u;
+        for (int i = tid; i < A.cells; i += blockDim.x) s_keys[i] = INF_KEY;
+    }
+    if (tid < 10) s_cnt[tid] = 0ull;
+    __syncthreads();
+
+    uint32_t* tile_counts = TILE ? s_counts : A.counts;
+    uint32_t* tile_keys = TILE ? s_keys : A.keys;
+
+    const int lane = tid & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+    Photon ph;
+    bool active = false;
+    int64_t k = 0;
+    int32_t seg = 0;
+    int64_t pool_lo = 0, pool_hi = 0, pool_src = 0;   // warp-uniform
+    bool exhausted = false;                           // warp-uniform
+    uint32_t n_det = 0, n_front = 0, n_bulk = 0, n_wall = 0, n_sipm = 0, n_cap = 0, n_sur = 0;
+    unsigned long long c_scat = 0, c_sumb = 0, c_steps = 0;
+    bool overrun = false;
+
+    for (;;) {
+        // ---- refill idle lanes from the warp's pool / the global queue ----
+        const unsigned need = __ballot_sync(FULL, !active);
+        if (need != 0u && !exhausted) {
+            const int nneed = __popc(need);
+            const int rank = __popc(need & lt_mask);
+            int64_t my_k = -1;
+            int64_t my_hint = pool_src;
+            const int64_t avail = pool_hi - pool_lo;
+            const int64_t taken = avail < nneed ? avail : (int64_t)nneed;
+            if (!active && rank < taken) my_k = pool_lo + rank;
+            pool_lo += taken;
+            if (taken < nneed) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(A.queue, (unsigned long long)A.warp_chunk);
+                base = __shfl_sync(FULL, base, 0);
+                if ((int64_t)base >= A.n) {
+                    exhausted = true;
+                } else {
+                    pool_lo = (int64_t)base;
+                    pool_hi = pool_lo + A.warp_chunk;
+                    if (pool_hi > A.n) pool_hi = A.n;
+                    if (MODE == 1) {
+                        int64_t s0 = 0;
+                        if (lane == 0) s0 = find_source(A.src_off, A.n_src, pool_src, pool_lo);
+                        pool_src = __shfl_sync(FULL, s0, 0);
+                    }
+                    const int64_t rem = nneed - taken;
+                    const int64_t avail2 = pool_hi - pool_lo;
+                    const int64_t taken2 = avail2 < rem ? avail2 : rem;
+                    if (!active && rank >= taken && rank - taken < taken2) {
+                        my_k = pool_lo + (rank - taken);
+                        my_hint = pool_src;
+                    }
+                    pool_lo += taken2;
+                }
+            }
+            if (my_k >= 0) {
+                k = my_k;
+                float sx, sy, sz, st;
+                if (MODE == 0) {
+                    const int32_t j = A.npos == 1 ? 0 : (int32_t)((uint64_t)k % (uint64_t)A.npos);
+                    sx = __ldg(A.px + j); sy = __ldg(A.py + j); sz = __ldg(A.pz + j);
+                    st = A.pt ? __ldg(A.pt + j) : 0.0f;
+                } else {
+                    const int64_t s = find_source(A.src_off, A.n_src, my_hint, k);
+                    sx = __ldg(A.px + s); sy = __ldg(A.py + s); sz = __ldg(A.pz + s);
+                    st = A.pt ? __ldg(A.pt + s) : 0.0f;
+                    seg = __ldg(A.src_seg + s);
+                }
+                photon_start(ph, P, s_tab, A.pid0 + (uint64_t)k + 1ull, sx, sy, sz, st);
+                active = true;
+            }
+        }
+        if (!__any_sync(FULL, active)) break;
+
+        // ---- one bounce-loop iteration per active lane ----
+        int32_t status = ST_FLYING, idx = 0;
+        if (active) {
+            stream_topup(ph.rng, P.key0, P.key1);
+            status = photon_step(ph, P, s_tab, idx, overrun);
+            c_steps += 1ull;
+        }
+
+        // ---- detections: warp-aggregated atomics ----
+        const bool det = status == ST_DETECTED;
+        const unsigned dmask = __ballot_sync(FULL, det);
+        if (det) {
+            const int32_t lin = idx < 0 ? -idx : idx;
+            const int32_t cell = lin - 1;
+            const uint32_t key = float_key(ph.t);
+            if (MODE == 0) {
+                const int32_t slot = cell + A.cells * time_bin0(ph.t, P);
+                const unsigned g = __match_any_sync(dmask, slot);
+                if (lane == __ffs(g) - 1) atomicAdd(tile_counts + slot, (uint32_t)__popc(g));
+                atomicMin(tile_keys + cell, key);
+            } else {
+                const unsigned long long slot =
+                    (unsigned long long)seg * (unsigned long long)A.cells + (unsigned long long)cell;
+                const unsigned g = __match_any_sync(dmask, slot);
+                if (lane == __ffs(g) - 1) atomicAdd(A.maps + slot, (uint32_t)__popc(g));
+                atomicMin(A.keys + slot, key);
+            }
+        }
+
+        // ---- terminal bookkeeping ----
+        if (status != ST_FLYING) {
+            switch (status) {
+            case ST_DETECTED:
+                n_det += 1u; c_sumb += (unsigned long long)ph.bounces;
+                if (idx < 0) n_front += 1u;
+                break;
+            case ST_ABS_BULK: n_bulk += 1u; break;
+            case ST_ABS_WALL: n_wall += 1u; break;
+            case ST_ABS_SIPM: n_sipm += 1u; break;
+            case ST_ABS_SUR:  n_sur += 1u; break;
+            default:          n_cap += 1u; break;
+            }
+            c_scat += (unsigned long long)ph.nscat;
+            if (REC) {
+                if (A.r_status) A.r_status[k] = (uint8_t)status;
+                if (A.r_idx) A.r_idx[k] = (int16_t)idx;
+                if (A.r_t) A.r_t[k] = ph.t;
+                if (A.r_bounces) A.r_bounces[k] = ph.bounces;
+            }
+            active = false;
+        }
+    }
+
+    // ---- CTA reduction of the counters ----
+    {
+        const uint32_t v0 = __reduce_add_sync(FULL, n_det);
+        const uint32_t v1 = __reduce_add_sync(FULL, n_front);
+        const uint32_t v2 = __reduce_add_sync(FULL, n_bulk);
+        const uint32_t v3 = __reduce_add_sync(FULL, n_wall);
+        const uint32_t v4 = __reduce_add_sync(FULL, n_sipm);
+        const uint32_t v5 = __reduce_add_sync(FULL, n_cap);
+        const uint32_t v6 = __reduce_add_sync(FULL, n_sur);
+        const unsigned long long v7 = warp_sum_u64(c_scat);
+        const unsigned long long v8 = warp_sum_u64(c_sumb);
+        const unsigned long long v9 = warp_sum_u64(c_steps);
+        if (lane == 0) {
+            if (v0) atomicAdd(&s_cnt[0], (unsigned long long)v0);
+            if (v1) atomicAdd(&s_cnt[1], (unsigned long long)v1);
+            if (v2) atomicAdd(&s_cnt[2], (unsigned long long)v2);
+            if (v3) atomicAdd(&s_cnt[3], (unsigned long long)v3);
+            if (v4) atomicAdd(&s_cnt[4], (unsigned long long)v4);
+            if (v5) atomicAdd(&s_cnt[5], (unsigned long long)v5);
+            if (v6) atomicAdd(&s_cnt[6], (unsigned long long)v6);
+            if (v7) atomicAdd(&s_cnt[7], v7);
+            if (v8) atomicAdd(&s_cnt[8], v8);
+            if (v9) atomicAdd(&s_cnt[9], v9);
+        }
+        if (overrun) atomicOr(A.err, 1u);
+    }
+    __syncthreads();
+
+    // ---- one coalesced flush per CTA ----
+    if (TILE) {
+        const int nt = A.cells * A.bins_total;
+        for (int i = tid; i < nt; i += blockDim.x) {
+            const uint32_t v = s_counts[i];
+            if (v) atomicAdd(A.counts + i, v);
+        }
+        for (int i = tid; i < A.cells; i += blockDim.x) {
+            const uint32_t kk = s_keys[i];
+            if (kk != INF_KEY) atomicMin(A.keys + i, kk);
+        }
+    }
+    if (tid < 9) {
+        const unsigned long long v = s_cnt[tid];
+        if (v) atomicAdd(A.counters + tid, v);
+    } else if (tid == 9) {
+        const unsigned long long v = s_cnt[9];
+        if (v) atomicAdd(A.steps, v);
+    }
+
+    if (MODE == 0) {
+        // last CTA decodes the first-time keys into Float32 in place
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) s_last = (atomicAdd(A.done, 1u) == gridDim.x - 1u) ? 1u : 0u;
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            for (int i = tid; i < A.cells; i += blockDim.x) {
+                const uint32_t kk = __ldcg(A.keys + i);
+                A.keys[i] = __float_as_uint(key_float(kk));
+            }
+        }
+    }
+}
+
+// Zero the outputs and the work queue before a launch.
+__global__ void init_kernel(uint32_t* counts, int64_t n_counts, uint32_t* keys, int64_t n_keys,
+                            unsigned long long* counters, unsigned long long* queue,
+                            unsigned long long* steps, unsigned int* done, unsigned int* err)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t i = i0; i < n_counts; i += stride) counts[i] = 0u;
+    for (int64_t i = i0; i < n_keys; i += stride) keys[i] = INF_KEY;
+    if (i0 < 9) counters[i0] = 0ull;
+    if (i0 == 0) { *queue = 0ull; *steps = 0ull; *done = 0u; *err = 0u; }
+}
+
+// Segment mode: decode tmin keys in place and sum npe per segment.
+__global__ void finalize_segments(const uint32_t* maps, uint32_t* keys, int32_t* npe,
+                                  int64_t n_seg, int32_t cells)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = n_seg * cells;
+    for (int64_t i = i0; i < total; i += stride) keys[i] = __float_as_uint(key_float(keys[i]));
+    for (int64_t s = i0; s < n_seg; s += stride) {
+        uint32_t acc = 0;
+        const uint32_t* m = maps + s * cells;
+        for (int c = 0; c < cells; ++c) acc += m[c];
+        npe[s] = (int32_t)acc;
+    }
+}
+
+__global__ void decode_keys_kernel(uint32_t* keys, int64_t n)
+{
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) keys[i] = __float_as_uint(key_float(keys[i]));
+}
+
+// ---- diagnostics ----
+__global__ void debug_math_kernel(int fn, const float* in, float* out, int64_t n)
+{
+    __shared__ double2 s_tab[CLM_LOG_NTAB];
+    for (int i = threadIdx.x; i < CLM_LOG_NTAB; i += blockDim.x)
+        s_tab[i] = make_double2(c_logtab[2 * i], c_logtab[2 * i + 1]);
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float x = in[i];
+        float r;
+        if (fn == 0) r = cl_logf(x, s_tab);
+        else if (fn == 1) r = cl_sinf(x);
+        else r = cl_cosf(x);
+        out[i] = r;
+    }
+}
+
+__global__ void debug_philox_kernel(int use_curand, const uint32_t* ctr, uint32_t* out, int64_t n,
+                                    uint32_t k0, uint32_t k1)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint4 c = make_uint4(ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3]);
+        uint4 o;
+        if (use_curand) o = curand_Philox4x32_10(c, make_uint2(k0, k1));
+        else o = philox4x32_10(c, k0, k1);
+        out[4 * i] = o.x; out[4 * i + 1] = o.y; out[4 * i + 2] = o.z; out[4 * i + 3] = o.w;
+    }
+}
+
+__global__ void debug_randu_kernel(float* out, int64_t n, int32_t n_per, uint32_t k0, uint32_t k1)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        Stream s;
+        stream_init(s, (uint64_t)i + 1ull);
+        for (int32_t j = 0; j < n_per; ++j) {
+            if ((j % 3) == 0) stream_topup(s, k0, k1);   // exercise both buffer paths
+            out[i * n_per + j] = randu(s, k0, k1);
+        }
+    }
+}
+
+}  // namespace cl
+
+// ===========================================================================
+// Host side
+// ===========================================================================
+using namespace cl;
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+struct cl_handle {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    char err[512] = {0};
+    DevBuf src, out, rec, scratch, dbg;
+    int ctas_per_sm = 0;
+    int threads = 256;
+    int warp_chunk = 64;
+    int64_t last_steps = 0;
+    int max_smem_optin = 0;
+};
+
+static thread_local char g_create_err[512];
+
+__attribute__((format(printf, 3, 4)))
+static int set_err(cl_handle* h, int code, const char* fmt, ...)
+{
+    if (h) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(h->err, sizeof h->err, fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+static int cuda_fail(cl_handle* h, cudaError_t e, const char* what)
+{
+    cudaGetLastError();  // clear sticky non-fatal error
+    return set_err(h, e == cudaErrorMemoryAllocation ? CL_ERR_OOM : CL_ERR_CUDA,
+                   "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(h, call, what)                                   \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail((h), e_, (what)); \
+    } while (0)
+
+static int ensure(cl_handle* h, DevBuf& b, size_t bytes)
+{
+    if (bytes <= b.cap) return CL_OK;
+    if (b.p) { cudaFree(b.p); b.p = nullptr; b.cap = 0; }
+    size_t want = bytes + bytes / 4 + 256;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(h, CL_ERR_OOM, "device allocation of %zu bytes failed", want);
+    }
+    b.cap = want;
+    return CL_OK;
+}
+
+static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+template <int MODE, bool REC, bool TILE>
+static void set_kernel_attrs(int smem_optin)
+{
+    cudaFuncSetAttribute(transport_kernel<MODE, REC, TILE>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin);
+}
+
+extern "C" {
+
+const char* cl_version(void) { return CL_VERSION_STRING; }
+int cl_abi_version(void) { return CL_ABI_VERSION; }
+
+int cl_create(cl_handle** out, int device)
+{
+    g_create_err[0] = 0;
+    if (!out) {
+        snprintf(g_create_err, sizeof g_create_err, "cl_create: null output pointer");
+        return CL_ERR_ARG;
+    }
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        snprintf(g_create_err, sizeof g_create_err, "cl_create: CUDA device %d unavailable (%s)",
+                 device, e != cudaSuccess ? cudaGetErrorString(e) : "no such device");
+        return e != cudaSuccess ? CL_ERR_CUDA : CL_ERR_ARG;
+    }
+    cl_handle* h = new (std::nothrow) cl_handle();
+    if (!h) {
+        snprintf(g_create_err, sizeof g_create_err, "cl_create: out of host memory");
+        return CL_ERR_OOM;
+    }
+    h->device = device;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&h->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        snprintf(g_create_err, sizeof g_create_err, "cl_create: %s", cudaGetErrorString(e));
+        delete h;
+        return CL_ERR_CUDA;
+    }
+    set_kernel_attrs<0, false, true>(h->max_smem_optin);
+    set_kernel_attrs<0, true, true>(h->max_smem_optin);
+    set_kernel_attrs<0, false, false>(h->max_smem_optin);
+    set_kernel_attrs<0, true, false>(h->max_smem_optin);
+    set_kernel_attrs<1, false, false>(h->max_smem_optin);
+    set_kernel_attrs<1, true, false>(h->max_smem_optin);
+    cudaGetLastError();
+    if (ensure(h, h->scratch, 64) != CL_OK) {
+        snprintf(g_create_err, sizeof g_create_err, "cl_create: %s", h->err);
+        cudaStreamDestroy(h->stream);
+        delete h;
+        return CL_ERR_OOM;
+    }
+    *out = h;
+    return CL_OK;
+}
+
+void cl_destroy(cl_handle* h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    DevBuf* bufs[] = {&h->src, &h->out, &h->rec, &h->scratch, &h->dbg};
+    for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+const char* cl_last_error(const cl_handle* h) { return h ? h->err : g_create_err; }
+
+int64_t cl_last_steps(const cl_handle* h) { return h ? h->last_steps : 0; }
+
+int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta, int warp_chunk)
+{
+    if (!h) return CL_ERR_STATE;
+    if (ctas_per_sm < 0 || ctas_per_sm > 32) return set_err(h, CL_ERR_ARG, "ctas_per_sm out of range");
+    if (threads_per_cta != 0 && (threads_per_cta < 32 || threads_per_cta > 256 || threads_per_cta % 32))
+        return set_err(h, CL_ERR_ARG, "threads_per_cta must be a multiple of 32 in [32, 256]");
+    if (warp_chunk != 0 && (warp_chunk < 32 || warp_chunk > (1 << 20)))
+        return set_err(h, CL_ERR_ARG, "warp_chunk must be in [32, 2^20]");
+    h->ctas_per_sm = ctas_per_sm;
+    h->threads = threads_per_cta ? threads_per_cta : 256;
+    h->warp_chunk = warp_chunk ? warp_chunk : 64;
+    return CL_OK;
+}
+
+}  // extern "C"
+
+// ---- argument validation shared by the entry points ----
+static int check_params(cl_handle* h, const cl_box* box, const cl_optical_params* op,
+                        const cl_readout* ro, const cl_time_binning* tb, float tau_ns)
+{
+    if (!box || !op || !ro || !tb) return set_err(h, CL_ERR_ARG, "null parameter struct");
+    for (int i = 0; i < 3; ++i)
+        if (!(box->L[i] > 0.0f) || !std::isfinite(box->L[i]))
+            return set_err(h, CL_ERR_ARG, "box sizes must be finite and positive");
+    if (ro->grid.nx < 1 || ro->grid.ny < 1 || (int64_t)ro->grid.nx * ro->grid.ny > 32767)
+        return set_err(h, CL_ERR_ARG, "SiPM grid must have 1 <= nx*ny <= 32767");
+    if (!(ro->grid.pitch_mm > 0.0f)) return set_err(h, CL_ERR_ARG, "pitch_mm must be positive");
+    if (tb->nbins < 0 || tb->nbins > (1 << 24) || !(tb->bin_ns > 0.0f))
+        return set_err(h, CL_ERR_ARG, "time binning needs bin_ns > 0 and 0 <= nbins <= 2^24");
+    if (!(op->n_crystal > 0.0f) || !(op->n_coupling > 0.0f))
+        return set_err(h, CL_ERR_ARG, "refractive indices must be positive");
+    if (std::isnan(op->abs_len_mm) || std::isnan(op->rayleigh_mm) || std::isnan(op->wrap_R) ||
+        std::isnan(op->sigma_alpha) || std::isnan(op->pde) || std::isnan(tau_ns) || std::isinf(tau_ns))
+        return set_err(h, CL_ERR_ARG, "NaN/Inf in optical parameters or tau_ns");
+    return CL_OK;
+}
+
+static Physics make_physics(const cl_box* box, const cl_optical_params* op, const cl_readout* ro,
+                            const cl_time_binning* tb, float tau_ns, int32_t max_bounces, uint64_t seed)
+{
+    Physics P;
+    memset(&P, 0, sizeof P);
+    P.L0 = box->L[0]; P.L1 = box->L[1]; P.L2 = box->L[2];
+    P.n_crystal = op->n_crystal; P.n_coupling = op->n_coupling;
+    P.abs_len = op->abs_len_mm; P.ray_len = op->rayleigh_mm;
+    P.wrap_R = op->wrap_R; P.sigma_alpha = op->sigma_alpha; P.pde = op->pde;
+    P.inv_v = op->n_crystal / 299.792458f;
+    P.cx = ro->cx; P.cy = ro->cy; P.r2 = ro->r2; P.sur_R = ro->sur_R;
+    P.pitch = ro->grid.pitch_mm; P.bin_ns = tb->bin_ns; P.tau = tau_ns;
+    P.nx = ro->grid.nx; P.ny = ro->grid.ny; P.nbins = tb->nbins; P.max_bounces = max_bounces;
+    P.key0 = (uint32_t)seed; P.key1 = (uint32_t)(seed >> 32);
+    P.abs_finite = std::isfinite(op->abs_len_mm) ? 1 : 0;
+    P.ray_finite = std::isfinite(op->rayleigh_mm) ? 1 : 0;
+    P.wrap_specular = op->wrap_specular ? 1 : 0;
+    P.air_gap = op->air_gap ? 1 : 0;
+    P.disc = ro->disc ? 1 : 0;
+    P.sur_specular = ro->sur_specular ? 1 : 0;
+    P.two_sided = ro->two_sided ? 1 : 0;
+    return P;
+}
+
+// Scratch words: [0] queue u64, [1] steps u64, [2] done u32 | err u32
+struct Scratch {
+    unsigned long long* queue;
+    unsigned long long* steps;
+    unsigned int* done;
+    unsigned int* err;
+};
+
+static Scratch scratch_of(cl_handle* h)
+{
+    unsigned long long* base = (unsigned long long*)h->scratch.p;
+    Scratch s;
+    s.queue = base;
+    s.steps = base + 1;
+    s.done = (unsigned int*)(base + 2);
+    s.err = s.done + 1;
+    return s;
+}
+
+template <int MODE, bool REC, bool TILE>
+static int launch_transport(cl_handle* h, const KArgs& a, size_t smem, cudaStream_t st)
+{
+    auto kern = transport_kernel<MODE, REC, TILE>;
+    int per_sm = 0;
+    CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, h->threads, smem), "occupancy");
+    if (per_sm < 1) return set_err(h, CL_ERR_ARG, "transport kernel does not fit on an SM (shared tile too large)");
+    if (h->ctas_per_sm > 0 && h->ctas_per_sm < per_sm) per_sm = h->ctas_per_sm;
+    int64_t grid = (int64_t)h->num_sms * per_sm;
+    // no more CTAs than warps' worth of first chunks
+    const int64_t warps_needed = (a.n + a.warp_chunk - 1) / a.warp_chunk;
+    const int64_t ctas_needed = (warps_needed + (h->threads / 32) - 1) / (h->threads / 32);
+    if (grid > ctas_needed) grid = ctas_needed > 0 ? ctas_needed : 1;
+    kern<<<(unsigned)grid, h->threads, smem, st>>>(a);
+    CK(h, cudaGetLastError(), "transport kernel launch");
+    return CL_OK;
+}
+
+static int enqueue_point(cl_handle* h, const Physics& P, const float* px, const float* py,
+                         const float* pz, const float* pt, int32_t npos, int64_t n, uint64_t pid0,
+                         uint32_t* counts, uint32_t* keys, unsigned long long* counters,
+                         const cl_records* rec, cudaStream_t st)
+{
+    const int cells = P.nx * P.ny;
+    const int bins_total = P.nbins + 1;
+    const int64_t n_counts = (int64_t)cells * bins_total;
+    Scratch s = scratch_of(h);
+    init_kernel<<<(unsigned)std::min<int64_t>((n_counts + 255) / 256 + 1, 4096), 256, 0, st>>>(
+        counts, n_counts, keys, cells, counters, s.queue, s.steps, s.done, s.err);
+    CK(h, cudaGetLastError(), "init kernel launch");
+    if (n == 0) {
+        // no photons: decode the +Inf keys into Float32 +Inf
+        decode_keys_kernel<<<1, 256, 0, st>>>(keys, cells);
+        CK(h, cudaGetLastError(), "decode launch");
+        return CL_OK;
+    }
+    KArgs a;
+    memset(&a, 0, sizeof a);
+    a.P = P; a.pid0 = pid0; a.n = n; a.npos = npos; a.warp_chunk = h->warp_chunk;
+    a.cells = cells; a.bins_total = bins_total;
+    a.px = px; a.py = py; a.pz = pz; a.pt = pt;
+    a.counts = counts; a.keys = keys; a.counters = counters;
+    const bool want_rec = rec && (rec->status || rec->idx || rec->t || rec->bounces);
+    if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
+    a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
+    const size_t tile_bytes = ((size_t)n_counts + cells) * sizeof(uint32_t);
+    const bool tile = LOGTAB_BYTES + tile_bytes <= (size_t)std::min(h->max_smem_optin, 160 * 1024);
+    const size_t smem = LOGTAB_BYTES + (tile ? tile_bytes : 0);
+    if (tile) return want_rec ? launch_transport<0, true, true>(h, a, smem, st)
+                              : launch_transport<0, false, true>(h, a, smem, st);
+    return want_rec ? launch_transport<0, true, false>(h, a, smem, st)
+                    : launch_transport<0, false, false>(h, a, smem, st);
+}
+
+static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, const float* sy,
+                            const float* sz, const float* sT, const int64_t* off, const int32_t* segid,
+                            int64_t n_src, int64_t n_seg, int64_t n, uint64_t pid0,
+                            uint32_t* maps, uint32_t* keys, int32_t* npe,
+                            unsigned long long* counters, const cl_records* rec, cudaStream_t st)
+{
+    const int cells = P.nx * P.ny;
+    const int64_t total = (int64_t)cells * n_seg;
+    Scratch s = scratch_of(h);
+    init_kernel<<<(unsigned)std::min<int64_t>((total + 255) / 256 + 1, 8192), 256, 0, st>>>(
+        maps, total, keys, total, counters, s.queue, s.steps, s.done, s.err);
+    CK(h, cudaGetLastError(), "init kernel launch");
+    if (n > 0) {
+        KArgs a;
+        memset(&a, 0, sizeof a);
+        a.P = P; a.pid0 = pid0; a.n = n; a.npos = 1; a.warp_chunk = h->warp_chunk;
+        a.cells = cells; a.bins_total = P.nbins + 1;
+        a.px = sx; a.py = sy; a.pz = sz; a.pt = sT;
+        a.src_off = off; a.src_seg = segid; a.n_src = n_src;
+        a.keys = keys; a.maps = maps; a.counters = counters;
+        const bool want_rec = rec && (rec->status || rec->idx || rec->t || rec->bounces);
+        if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
+        a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
+        const int rc = want_rec ? launch_transport<1, true, false>(h, a, LOGTAB_BYTES, st)
+                                : launch_transport<1, false, false>(h, a, LOGTAB_BYTES, st);
+        if (rc != CL_OK) return rc;
+    }
+    finalize_segments<<<(unsigned)std::min<int64_t>((total + 255) / 256 + 1, 8192), 256, 0, st>>>(
+        maps, keys, npe, n_seg, cells);
+    CK(h, cudaGetLastError(), "finalize launch");
+    return CL_OK;
+}
+
+static int collect(cl_handle* h, cudaStream_t st)
+{
+    Scratch s = scratch_of(h);
+    unsigned long long steps = 0;
+    unsigned int err = 0;
+    CK(h, cudaMemcpyAsync(&steps, s.steps, sizeof steps, cudaMemcpyDeviceToHost, st), "copy steps");
+    CK(h, cudaMemcpyAsync(&err, s.err, sizeof err, cudaMemcpyDeviceToHost, st), "copy status");
+    CK(h, cudaStreamSynchronize(st), "stream synchronize");
+    h->last_steps = (int64_t)steps;
+    if (err) return set_err(h, CL_ERR_TIMEOUT, "a device-side loop budget ran out (Rayleigh rejection sampler)");
+    return CL_OK;
+}
+
+extern "C" {
+
+int cl_run_photons(cl_handle* h, const cl_box* box, const cl_optical_params* op,
+                   const cl_readout* ro, const cl_time_binning* tb,
+                   const float* px, const float* py, const float* pz,
+                   const float* pt, int32_t npos,
+                   int64_t n_photons, uint64_t seed, uint64_t pid_offset,
+                   float tau_ns, int32_t max_bounces,
+                   uint32_t* counts, float* first_ns, cl_counters* counters,
+                   const cl_records* records)
+{
+    if (!h) return CL_ERR_STATE;
+    h->err[0] = 0;
+    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    if (rc != CL_OK) return rc;
+    if (npos < 1 || !px || !py || !pz) return set_err(h, CL_ERR_ARG, "need npos >= 1 source positions");
+    if (n_photons < 0) return set_err(h, CL_ERR_ARG, "n_photons must be >= 0");
+    if (!counts || !first_ns || !counters) return set_err(h, CL_ERR_ARG, "null output buffer");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    cudaStream_t st = h->stream;
+
+    const int cells = ro->grid.nx * ro->grid.ny;
+    const size_t n_counts = (size_t)cells * (size_t)(tb->nbins + 1);
+    // device layout: sources | counts | keys | counters ; records separately
+    const size_t b_src = align256(4 * (size_t)npos * sizeof(float));
+    const size_t b_counts = align256(n_counts * sizeof(uint32_t));
+    const size_t b_keys = align256((size_t)cells * sizeof(uint32_t));
+    const size_t b_ctr = align256(sizeof(cl_counters));
+    if ((rc = ensure(h, h->src, b_src)) != CL_OK) return rc;
+    if ((rc = ensure(h, h->out, b_counts + b_keys + b_ctr)) != CL_OK) return rc;
+    float* d_px = (float*)h->src.p;
+    float* d_py = d_px + npos;
+    float* d_pz = d_py + npos;
+    float* d_pt = d_pz + npos;
+    uint32_t* d_counts = (uint32_t*)h->out.p;
+    uint32_t* d_keys = (uint32_t*)((char*)h->out.p + b_counts);
+    unsigned long long* d_ctr = (unsigned long long*)((char*)h->out.p + b_counts + b_keys);
+
+    cl_records drec;
+    memset(&drec, 0, sizeof drec);
+    const bool want_rec = records && (records->status || records->idx || records->t || records->bounces);
+    if (want_rec && n_photons > 0) {
+        const size_t n = (size_t)n_photons;
+        const size_t b1 = align256(n), b2 = align256(2 * n), b4 = align256(4 * n);
+        if ((rc = ensure(h, h->rec, b1 + b2 + 2 * b4)) != CL_OK) return rc;
+        char* base = (char*)h->rec.p;
+        if (records->status) drec.status = (uint8_t*)base;
+        if (records->idx) drec.idx = (int16_t*)(base + b1);
+        if (records->t) drec.t = (float*)(base + b1 + b2);
+        if (records->bounces) drec.bounces = (int32_t*)(base + b1 + b2 + b4);
+    }
+
+    CK(h, cudaMemcpyAsync(d_px, px, npos * sizeof(float), cudaMemcpyHostToDevice, st), "copy px");
+    CK(h, cudaMemcpyAsync(d_py, py, npos * sizeof(float), cudaMemcpyHostToDevice, st), "copy py");
+    CK(h, cudaMemcpyAsync(d_pz, pz, npos * sizeof(float), cudaMemcpyHostToDevice, st), "copy pz");
+    if (pt) CK(h, cudaMemcpyAsync(d_pt, pt, npos * sizeof(float), cudaMemcpyHostToDevice, st), "copy pt");
+
+    const Physics P = make_physics(box, op, ro, tb, tau_ns, max_bounces, seed);
+    rc = enqueue_point(h, P, d_px, d_py, d_pz, pt ? d_pt : nullptr, npos, n_photons, pid_offset,
+                       d_counts, d_keys, d_ctr, want_rec ? &drec : nullptr, st);
+    if (rc != CL_OK) return rc;
+
+    CK(h, cudaMemcpyAsync(counts, d_counts, n_counts * sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "copy counts");
+    CK(h, cudaMemcpyAsync(first_ns, d_keys, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, st), "copy first_ns");
+    CK(h, cudaMemcpyAsync(counters, d_ctr, sizeof(cl_counters), cudaMemcpyDeviceToHost, st), "copy counters");
+    if (want_rec && n_photons > 0) {
+        const size_t n = (size_t)n_photons;
+        if (records->status) CK(h, cudaMemcpyAsync(records->status, drec.status, n, cudaMemcpyDeviceToHost, st), "copy status");
+        if (records->idx) CK(h, cudaMemcpyAsync(records->idx, drec.idx, 2 * n, cudaMemcpyDeviceToHost, st), "copy idx");
+        if (records->t) CK(h, cudaMemcpyAsync(records->t, drec.t, 4 * n, cudaMemcpyDeviceToHost, st), "copy t");
+        if (records->bounces) CK(h, cudaMemcpyAsync(records->bounces, drec.bounces, 4 * n, cudaMemcpyDeviceToHost, st), "copy bounces");
+    }
+    return collect(h, st);
+}
+
+int cl_run_photons_device(cl_handle* h, const cl_box* box, const cl_optical_params* op,
+                          const cl_readout* ro, const cl_time_binning* tb,
+                          const float* d_px, const float* d_py, const float* d_pz,
+                          const float* d_pt, int32_t npos,
+                          int64_t n_photons, uint64_t seed, uint64_t pid_offset,
+                          float tau_ns, int32_t max_bounces,
+                          uint32_t* d_counts, float* d_first_ns,
+                          cl_counters* d_counters, const cl_records* d_records, void* stream)
+{
+    if (!h) return CL_ERR_STATE;
+    h->err[0] = 0;
+    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    if (rc != CL_OK) return rc;
+    if (npos < 1 || !d_px || !d_py || !d_pz) return set_err(h, CL_ERR_ARG, "need npos >= 1 source positions");
+    if (n_photons < 0) return set_err(h, CL_ERR_ARG, "n_photons must be >= 0");
+    if (!d_counts || !d_first_ns || !d_counters) return set_err(h, CL_ERR_ARG, "null output buffer");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    const Physics P = make_physics(box, op, ro, tb, tau_ns, max_bounces, seed);
+    return enqueue_point(h, P, d_px, d_py, d_pz, d_pt, npos, n_photons, pid_offset, d_counts,
+                         (uint32_t*)d_first_ns, (unsigned long long*)d_counters, d_records, st);
+}
+
+static int check_segments(cl_handle* h, const int64_t* off, const int32_t* seg, int64_t n_src,
+                          int64_t n_seg, int64_t* total)
+{
+    if (n_src < 1 || n_seg < 1) return set_err(h, CL_ERR_ARG, "need n_src >= 1 and n_segments >= 1");
+    if (!off || !seg) return set_err(h, CL_ERR_ARG, "null source offsets or segment ids");
+    if (off[0] != 0) return set_err(h, CL_ERR_ARG, "src_offsets[0] must be 0");
+    for (int64_t s = 0; s < n_src; ++s) {
+        if (off[s + 1] < off[s]) return set_err(h, CL_ERR_ARG, "src_offsets must be non-decreasing");
+        if (seg[s] < 0 || seg[s] >= n_seg) return set_err(h, CL_ERR_ARG, "segment id out of range");
+        if (s > 0 && seg[s] < seg[s - 1]) return set_err(h, CL_ERR_ARG, "segment ids must be non-decreasing");
+    }
+    *total = off[n_src];
+    return CL_OK;
+}
+
+int cl_run_segments(cl_handle* h, const cl_box* box, const cl_optical_params* op,
+                    const cl_readout* ro, const cl_time_binning* tb,
+                    const float* sx, const float* sy, const float* sz,
+                    const float* st_, const int64_t* src_offsets,
+                    const int32_t* src_segment, int64_t n_src, int64_t n_segments,
+                    uint64_t seed, uint64_t pid_offset,
+                    float tau_ns, int32_t max_bounces,
+                    uint32_t* maps, float* tmin, int32_t* npe,
+                    cl_counters* counters, const cl_records* records)
+{
+    if (!h) return CL_ERR_STATE;
+    h->err[0] = 0;
+    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    if (rc != CL_OK) return rc;
+    int64_t n = 0;
+    if ((rc = check_segments(h, src_offsets, src_segment, n_src, n_segments, &n)) != CL_OK) return rc;
+    if (!sx || !sy || !sz) return set_err(h, CL_ERR_ARG, "null source positions");
+    if (!maps || !tmin || !npe || !counters) return set_err(h, CL_ERR_ARG, "null output buffer");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    cudaStream_t st = h->stream;
+    const int cells = ro->grid.nx * ro->grid.ny;
+    const size_t total = (size_t)cells * (size_t)n_segments;
+    const size_t b_f = align256((size_t)n_src * sizeof(float));
+    const size_t b_off = align256((size_t)(n_src + 1) * sizeof(int64_t));
+    const size_t b_seg = align256((size_t)n_src * sizeof(int32_t));
+    const size_t b_maps = align256(total * sizeof(uint32_t));
+    const size_t b_npe = align256((size_t)n_segments * sizeof(int32_t));
+    const size_t b_ctr = align256(sizeof(cl_counters));
+    if ((rc = ensure(h, h->src, 4 * b_f + b_off + b_seg)) != CL_OK) return rc;
+    if ((rc = ensure(h, h->out, 2 * b_maps + b_npe + b_ctr)) != CL_OK) return rc;
+    char* sb = (char*)h->src.p;
+    float* d_sx = (float*)sb;
+    float* d_sy = (float*)(sb + b_f);
+    float* d_sz = (float*)(sb + 2 * b_f);
+    float* d_st = (float*)(sb + 3 * b_f);
+    int64_t* d_off = (int64_t*)(sb + 4 * b_f);
+    int32_t* d_seg = (int32_t*)(sb + 4 * b_f + b_off);
+    char* ob = (char*)h->out.p;
+    uint32_t* d_maps = (uint32_t*)ob;
+    uint32_t* d_keys = (uint32_t*)(ob + b_maps);
+    int32_t* d_npe = (int32_t*)(ob + 2 * b_maps);
+    unsigned long long* d_ctr = (unsigned long long*)(ob + 2 * b_maps + b_npe);
+
+    cl_records drec;
+    memset(&drec, 0, sizeof drec);
+    const bool want_rec = records && (records->status || records->idx || records->t || records->bounces);
+    if (want_rec && n > 0) {
+        const size_t m = (size_t)n;
+        const size_t b1 = align256(m), b2 = align256(2 * m), b4 = align256(4 * m);
+        if ((rc = ensure(h, h->rec, b1 + b2 + 2 * b4)) != CL_OK) return rc;
+        char* base = (char*)h->rec.p;
+        if (records->status) drec.status = (uint8_t*)base;
+        if (records->idx) drec.idx = (int16_t*)(base + b1);
+        if (records->t) drec.t = (float*)(base + b1 + b2);
+        if (records->bounces) drec.bounces = (int32_t*)(base + b1 + b2 + b4);
+    }
+    const size_t fs = (size_t)n_src * sizeof(float);
+    CK(h, cudaMemcpyAsync(d_sx, sx, fs, cudaMemcpyHostToDevice, st), "copy sx");
+    CK(h, cudaMemcpyAsync(d_sy, sy, fs, cudaMemcpyHostToDevice, st), "copy sy");
+    CK(h, cudaMemcpyAsync(d_sz, sz, fs, cudaMemcpyHostToDevice, st), "copy sz");
+    if (st_) CK(h, cudaMemcpyAsync(d_st, st_, fs, cudaMemcpyHostToDevice, st), "copy st");
+    CK(h, cudaMemcpyAsync(d_off, src_offsets, (size_t)(n_src + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st), "copy offsets");
+    CK(h, cudaMemcpyAsync(d_seg, src_segment, (size_t)n_src * sizeof(int32_t), cudaMemcpyHostToDevice, st), "copy segments");
+
+    const Physics P = make_physics(box, op, ro, tb, tau_ns, max_bounces, seed);
+    rc = enqueue_segments(h, P, d_sx, d_sy, d_sz, st_ ? d_st : nullptr, d_off, d_seg, n_src, n_segments,
+                          n, pid_offset, d_maps, d_keys, d_npe, d_ctr, want_rec ? &drec : nullptr, st);
+    if (rc != CL_OK) return rc;
+    CK(h, cudaMemcpyAsync(maps, d_maps, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "copy maps");
+    CK(h, cudaMemcpyAsync(tmin, d_keys, total * sizeof(float), cudaMemcpyDeviceToHost, st), "copy tmin");
+    CK(h, cudaMemcpyAsync(npe, d_npe, (size_t)n_segments * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "copy npe");
+    CK(h, cudaMemcpyAsync(counters, d_ctr, sizeof(cl_counters), cudaMemcpyDeviceToHost, st), "copy counters");
+    if (want_rec && n > 0) {
+        const size_t m = (size_t)n;
+        if (records->status) CK(h, cudaMemcpyAsync(records->status, drec.status, m, cudaMemcpyDeviceToHost, st), "copy status");
+        if (records->idx) CK(h, cudaMemcpyAsync(records->idx, drec.idx, 2 * m, cudaMemcpyDeviceToHost, st), "copy idx");
+        if (records->t) CK(h, cudaMemcpyAsync(records->t, drec.t, 4 * m, cudaMemcpyDeviceToHost, st), "copy t");
+        if (records->bounces) CK(h, cudaMemcpyAsync(records->bounces, drec.bounces, 4 * m, cudaMemcpyDeviceToHost, st), "copy bounces");
+    }
+    return collect(h, st);
+}
+
+int cl_run_segments_device(cl_handle* h, const cl_box* box, const cl_optical_params* op,
+                           const cl_readout* ro, const cl_time_binning* tb,
+                           const float* d_sx, const float* d_sy, const float* d_sz,
+                           const float* d_st, const int64_t* d_src_offsets,
+                           const int32_t* d_src_segment, int64_t n_src, int64_t n_segments,
+                           int64_t n_photons, uint64_t seed, uint64_t pid_offset,
+                           float tau_ns, int32_t max_bounces,
+                           uint32_t* d_maps, float* d_tmin, int32_t* d_npe,
+                           cl_counters* d_counters, const cl_records* d_records, void* stream)
+{
+    if (!h) return CL_ERR_STATE;
+    h->err[0] = 0;
+    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    if (rc != CL_OK) return rc;
+    if (n_src < 1 || n_segments < 1) return set_err(h, CL_ERR_ARG, "need n_src >= 1 and n_segments >= 1");
+    if (!d_sx || !d_sy || !d_sz || !d_src_offsets || !d_src_segment)
+        return set_err(h, CL_ERR_ARG, "null source array");
+    if (!d_maps || !d_tmin || !d_npe || !d_counters) return set_err(h, CL_ERR_ARG, "null output buffer");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    const int64_t n = n_photons;
+    if (n < 0) return set_err(h, CL_ERR_ARG, "negative photon total");
+    const Physics P = make_physics(box, op, ro, tb, tau_ns, max_bounces, seed);
+    return enqueue_segments(h, P, d_sx, d_sy, d_sz, d_st, d_src_offsets, d_src_segment, n_src, n_segments,
+                            n, pid_offset, d_maps, (uint32_t*)d_tmin, d_npe,
+                            (unsigned long long*)d_counters, d_records, st);
+}
+
+int cl_sync(cl_handle* h, void* stream)
+{
+    if (!h) return CL_ERR_STATE;
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    return collect(h, stream ? (cudaStream_t)stream : h->stream);
+}
+
+int cl_debug_eval(cl_handle* h, int fn, const void* in, void* out, int64_t n, uint64_t seed, int32_t n_per)
+{
+    if (!h) return CL_ERR_STATE;
+    h->err[0] = 0;
+    if (n < 0 || !out || (fn != 4 && !in)) return set_err(h, CL_ERR_ARG, "bad debug arguments");
+    if (fn < 0 || fn > 5) return set_err(h, CL_ERR_ARG, "unknown debug function");
+    if (fn == 4 && n_per < 1) return set_err(h, CL_ERR_ARG, "n_per must be >= 1");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    cudaStream_t st = h->stream;
+    size_t in_b = 0, out_b = 0;
+    if (fn <= 2) { in_b = 4 * (size_t)n; out_b = 4 * (size_t)n; }
+    else if (fn == 3 || fn == 5) { in_b = 16 * (size_t)n; out_b = 16 * (size_t)n; }
+    else { out_b = 4 * (size_t)n * (size_t)n_per; }
+    int rc = ensure(h, h->dbg, align256(in_b) + align256(out_b) + 256);
+    if (rc != CL_OK) return rc;
+    char* din = (char*)h->dbg.p;
+    char* dout = din + align256(in_b);
+    if (in_b) CK(h, cudaMemcpyAsync(din, in, in_b, cudaMemcpyHostToDevice, st), "copy in");
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    if (n > 0) {
+        if (fn <= 2) debug_math_kernel<<<grid, 256, 0, st>>>(fn, (const float*)din, (float*)dout, n);
+        else if (fn == 3 || fn == 5)
+            debug_philox_kernel<<<grid, 256, 0, st>>>(fn == 5, (const uint32_t*)din, (uint32_t*)dout, n, k0, k1);
+        else debug_randu_kernel<<<grid, 256, 0, st>>>((float*)dout, n, n_per, k0, k1);
+        CK(h, cudaGetLastError(), "debug kernel launch");
+    }
+    if (out_b) CK(h, cudaMemcpyAsync(out, dout, out_b, cudaMemcpyDeviceToHost, st), "copy out");
+    CK(h, cudaStreamSynchronize(st), "stream synchronize");
+    return CL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,267 @@
+/*
+ * crysplight_cuda.h — C-ABI of the B200 optical-photon transport engine.
+ *
+ * Drop-in boundary for CryspLight's transport call.  The reference has no FFI:
+ * its seam is the Julia function
+ *
+ *   run_photons_ka!(box, op, ro, tb; n_photons, seed, pos | positions, t0s,
+ *                   pid_offset, tau_ns, max_bounces, ArrayT, return_records)
+ *       -> Accumulator [, records]                      (src/kernel.jl:312-367)
+ *
+ * and its CPU twin run_photons! (src/transport.jl:245-273).  The entry points
+ * below take the same arguments as plain pointers and sizes, so a Julia
+ * `ccall` (or ctypes, or C) binds them directly.  The parameter structs are
+ * layout-identical to the Julia isbits structs (C rules, Bool = uint8_t), so a
+ * Julia `Ref(op)` can be passed where a `const cl_optical_params*` is expected.
+ *
+ * Conventions (kept from the reference):
+ *   - photon ids are 1-based: the k-th photon of a call (k = 0..n-1) draws
+ *     from the Philox4x32-10 stream key = (seed lo, seed hi),
+ *     counter = (pid lo, pid hi, block, 0) with pid = pid_offset + k + 1
+ *     (src/philox.jl:30-48, src/kernel.jl:163);
+ *   - the source of photon k is positions[k % npos] (src/kernel.jl:173);
+ *   - counts are column-major (nx, ny, nbins+1): counts[i + nx*(j + ny*bin)],
+ *     so a Julia Array{UInt32,3} aliases them (src/transport.jl:64-80);
+ *   - the record index idx = (jj-1)*nx + ii is 1-based and negative for a
+ *     detection on the z = 0 face (src/kernel.jl:232-235).
+ *
+ * Ownership: the caller owns every host buffer; the library owns device
+ * buffers and a CUDA stream inside the opaque handle and reuses them across
+ * calls.  No pointer is retained after a call returns.  A handle is not
+ * re-entrant: use one handle per host thread.  Errors are returned as
+ * negative codes with a message from cl_last_error(); the library never
+ * aborts the process.
+ */
+#ifndef CRYSPLIGHT_CUDA_H
+#define CRYSPLIGHT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CL_ABI_VERSION 1
+
+/* Photon fates, src/transport.jl:6-12. */
+#define CL_STATUS_DETECTED 1
+#define CL_STATUS_ABS_BULK 2
+#define CL_STATUS_ABS_WALL 3
+#define CL_STATUS_ABS_SIPM 4
+#define CL_STATUS_CAP      5
+#define CL_STATUS_ABS_SUR  6
+
+/* Return codes.  The reference raises Julia exceptions instead. */
+#define CL_OK            0
+#define CL_ERR_ARG      -1   /* invalid argument (reference: ArgumentError/BoundsError) */
+#define CL_ERR_CUDA     -2   /* CUDA runtime failure                                    */
+#define CL_ERR_OOM      -3   /* device allocation failed                                */
+#define CL_ERR_TIMEOUT  -4   /* a device-side loop budget ran out                       */
+#define CL_ERR_STATE    -5   /* handle misuse (null handle, wrong device)               */
+
+/* Box, src/geometry.jl:14-16: crystal [0,L0]x[0,L1]x[0,L2] in mm. */
+typedef struct cl_box {
+    float L[3];
+} cl_box;
+
+/* OpticalParams, src/transport.jl:14-24 (32 bytes). */
+typedef struct cl_optical_params {
+    float   n_crystal;
+    float   n_coupling;
+    float   abs_len_mm;     /* +Inf disables bulk absorption     */
+    float   rayleigh_mm;    /* +Inf disables Rayleigh scattering */
+    float   wrap_R;
+    uint8_t wrap_specular;  /* 1 = ESR (specular), 0 = PTFE (Lambertian) */
+    uint8_t air_gap;        /* 1 = back-painted, 0 = front-painted      */
+    float   sigma_alpha;    /* UNIFIED roughness, radians               */
+    float   pde;
+} cl_optical_params;
+
+/* SipmGrid, src/transport.jl:26-30 (12 bytes). */
+typedef struct cl_sipm_grid {
+    float   pitch_mm;
+    int32_t nx;
+    int32_t ny;
+} cl_sipm_grid;
+
+/* Readout, src/transport.jl:41-50 (36 bytes). */
+typedef struct cl_readout {
+    cl_sipm_grid grid;
+    uint8_t disc;           /* 1 = only a disc of radius sqrt(r2) about (cx,cy) is active */
+    float   cx;
+    float   cy;
+    float   r2;
+    float   sur_R;
+    uint8_t sur_specular;
+    uint8_t two_sided;      /* sensors on both z faces */
+} cl_readout;
+
+/* TimeBinning, src/transport.jl:59-62: counts have nbins+1 bins, the last one overflow. */
+typedef struct cl_time_binning {
+    float   bin_ns;
+    int32_t nbins;
+} cl_time_binning;
+
+/* Scalar fields of Accumulator, src/transport.jl:64-76, same order. */
+typedef struct cl_counters {
+    int64_t ndet;
+    int64_t ndet_front;
+    int64_t nabs_bulk;
+    int64_t nabs_wall;
+    int64_t nabs_sipm;
+    int64_t ncap;
+    int64_t nabs_sur;
+    int64_t nscat;
+    int64_t sum_bounces_det;
+} cl_counters;
+
+/* Per-photon records of transport_kernel!, src/kernel.jl:159-161,300-303
+ * (11 bytes per photon).  Any pointer may be NULL to skip that field. */
+typedef struct cl_records {
+    uint8_t* status;
+    int16_t* idx;
+    float*   t;
+    int32_t* bounces;
+} cl_records;
+
+typedef struct cl_handle cl_handle;
+
+/* Library version string and ABI version (CL_ABI_VERSION). */
+const char* cl_version(void);
+int cl_abi_version(void);
+
+/* Create a handle bound to CUDA device `device`.  The reference's equivalent
+ * is the backend choice ArrayT / KA.get_backend (src/kernel.jl:330). */
+int cl_create(cl_handle** out, int device);
+void cl_destroy(cl_handle* h);
+/* Message of the last failing call on this handle ("" if none).  With a NULL
+ * handle, the message of the last failing cl_create on this thread. */
+const char* cl_last_error(const cl_handle* h);
+
+/*
+ * Point-source / position-scan transport with host buffers — the replacement
+ * for run_photons_ka!(...) (src/kernel.jl:312-367) and, for pid_offset = 0 and
+ * pt = NULL, for run_photons! (src/transport.jl:245-273).
+ *
+ *   px,py,pz   npos source positions (mm); photon k starts at position k % npos
+ *   pt         npos emission-time offsets (ns), or NULL for zeros (t0s)
+ *   n_photons  number of photons; pid = pid_offset + k + 1
+ *   tau_ns     exponential emission time constant, 0 = delta
+ *   counts     out: nx*ny*(nbins+1) uint32, column-major (overwritten)
+ *   first_ns   out: nx*ny float, earliest detection per SiPM, +Inf if none
+ *   counters   out: Accumulator counters
+ *   records    optional per-photon records (host arrays of n_photons), or NULL
+ *
+ * Synchronous.  Results are bit-identical for any launch configuration.
+ */
+int cl_run_photons(cl_handle* h,
+                   const cl_box* box, const cl_optical_params* op,
+                   const cl_readout* ro, const cl_time_binning* tb,
+                   const float* px, const float* py, const float* pz,
+                   const float* pt, int32_t npos,
+                   int64_t n_photons, uint64_t seed, uint64_t pid_offset,
+                   float tau_ns, int32_t max_bounces,
+                   uint32_t* counts, float* first_ns, cl_counters* counters,
+                   const cl_records* records);
+
+/*
+ * Same as cl_run_photons with every pointer in device memory, enqueued on
+ * `stream` (a cudaStream_t; NULL = the handle's own stream) without a host
+ * synchronisation.  `counters` is device memory too.  Call cl_sync() to wait
+ * and to collect device-side errors.
+ */
+int cl_run_photons_device(cl_handle* h,
+                          const cl_box* box, const cl_optical_params* op,
+                          const cl_readout* ro, const cl_time_binning* tb,
+                          const float* d_px, const float* d_py, const float* d_pz,
+                          const float* d_pt, int32_t npos,
+                          int64_t n_photons, uint64_t seed, uint64_t pid_offset,
+                          float tau_ns, int32_t max_bounces,
+                          uint32_t* d_counts, float* d_first_ns,
+                          cl_counters* d_counters, const cl_records* d_records,
+                          void* stream);
+
+/*
+ * Segmented transport: many sources, each emitting its own number of photons,
+ * grouped into segments (points of a scan, or 511 keV events).  This is the
+ * batched form of the event pipeline's flush! (src/events.jl:65-91) and of a
+ * per-point scan (one run_photons_ka! call per point with pid_offset =
+ * photons before it): photons are numbered source-major, photon k (0-based,
+ * over the whole call) has pid = pid_offset + k + 1 and belongs to the source
+ * s with src_offsets[s] <= k < src_offsets[s+1], starting at
+ * (sx,sy,sz)[s] with emission offset st[s] (NULL = 0).
+ *
+ *   src_offsets  n_src+1 non-decreasing int64 prefix sums, src_offsets[0] = 0
+ *   src_segment  n_src segment ids in [0, n_segments), non-decreasing
+ *   maps         out: nx*ny*n_segments uint32, time-integrated detected counts
+ *                per segment, maps[i + nx*(j + ny*seg)] (events.jl: maps[ii,jj,ev])
+ *   tmin         out: nx*ny*n_segments float, first detection time, +Inf if none
+ *   npe          out: n_segments int32, detections per segment
+ *   counters     out: totals over the call
+ *   records      optional, per photon, indexed by k
+ *
+ * Host buffers, synchronous.  `tb` is accepted for interface symmetry; the
+ * per-segment maps are time-integrated as in the event pipeline.
+ */
+int cl_run_segments(cl_handle* h,
+                    const cl_box* box, const cl_optical_params* op,
+                    const cl_readout* ro, const cl_time_binning* tb,
+                    const float* sx, const float* sy, const float* sz,
+                    const float* st, const int64_t* src_offsets,
+                    const int32_t* src_segment, int64_t n_src, int64_t n_segments,
+                    uint64_t seed, uint64_t pid_offset,
+                    float tau_ns, int32_t max_bounces,
+                    uint32_t* maps, float* tmin, int32_t* npe,
+                    cl_counters* counters, const cl_records* records);
+
+/* Device-memory, asynchronous form of cl_run_segments (see
+ * cl_run_photons_device).  n_photons must equal d_src_offsets[n_src]; the
+ * offsets and segment ids are trusted (the host form validates them). */
+int cl_run_segments_device(cl_handle* h,
+                           const cl_box* box, const cl_optical_params* op,
+                           const cl_readout* ro, const cl_time_binning* tb,
+                           const float* d_sx, const float* d_sy, const float* d_sz,
+                           const float* d_st, const int64_t* d_src_offsets,
+                           const int32_t* d_src_segment, int64_t n_src,
+                           int64_t n_segments, int64_t n_photons,
+                           uint64_t seed, uint64_t pid_offset,
+                           float tau_ns, int32_t max_bounces,
+                           uint32_t* d_maps, float* d_tmin, int32_t* d_npe,
+                           cl_counters* d_counters, const cl_records* d_records,
+                           void* stream);
+
+/* Wait for the work enqueued by the *_device calls on `stream` (NULL = the
+ * handle's stream) and report device-side errors (CL_ERR_TIMEOUT). */
+int cl_sync(cl_handle* h, void* stream);
+
+/*
+ * Number of transport-loop iterations ("photon-steps": wall interactions,
+ * Rayleigh scatters and terminal steps) executed by the last completed call on
+ * this handle.  Diagnostic for throughput per step; 0 if not available.
+ */
+int64_t cl_last_steps(const cl_handle* h);
+
+/*
+ * Launch shape used by the transport kernels: CTAs per SM and threads per CTA
+ * (0 = automatic), and the number of photons a warp claims from the device
+ * work queue at a time.  Results do not depend on these values.
+ */
+int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta,
+                  int warp_chunk);
+
+/*
+ * Diagnostics for tests: evaluate the device's Float32 elementary functions
+ * on n inputs.  fn: 0 = log, 1 = sin, 2 = cos, 3 = Philox4x32-10 on
+ * (in_u32[4k..4k+3] counter, key = (seed lo, hi)) -> out_u32[4k..4k+3],
+ * 4 = randu stream: out[k*m + i] = i-th uniform of pid = k + 1 (m = n_per).
+ * Host buffers, synchronous.
+ */
+int cl_debug_eval(cl_handle* h, int fn, const void* in, void* out, int64_t n,
+                  uint64_t seed, int32_t n_per);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CRYSPLIGHT_CUDA_H */

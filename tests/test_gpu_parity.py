@@ -1,0 +1,302 @@
+"""Parity of the sm_100a CUDA library with the CPU oracle, through the C-ABI.
+
+Integer/bit-level outputs (Philox, uniforms, per-photon records, count maps,
+first-hit times) are compared for exact equality; the transport's per-photon
+fate agreement must be >= 99.9% (the target the reference sets for a GPU
+twin whose transcendentals may differ by an ulp) and is reported.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from crysplight_b200.params import (Box, OpticalParams, Readout, SipmGrid, TimeBinning,
+                                    deg2rad_f32)
+from cases import (BOX_BGO, BOX_CSI, CENTRE_BGO, CENTRE_CSI, GRID, INF, OP_ALL, OP_BENCH, OP_C1,
+                   OP_C2, RO_ALL, TAU_C1, TAU_C2, TB, TB80, ideal, scan_points)
+
+pytestmark = pytest.mark.gpu
+NT = os.cpu_count() or 1
+
+
+def _fate_report(a, b):
+    """Per-photon fate agreement (status and signed SiPM index)."""
+    same_fate = (a.status == b.status) & (a.idx == b.idx)
+    exact = same_fate & (a.bounces == b.bounces) & (a.t.view(np.uint32) == b.t.view(np.uint32))
+    n = a.status.size
+    return same_fate.sum() / max(n, 1), int(n - exact.sum())
+
+
+def _assert_records_equal(dev, ref, min_fate=0.999):
+    fate, nonexact = _fate_report(dev, ref)
+    print(f"fate agreement {fate:.7f}, non-identical records {nonexact}")
+    assert fate >= min_fate
+    return nonexact
+
+
+def _assert_acc_equal(a, b):
+    assert np.array_equal(a.counts, b.counts)
+    assert np.array_equal(a.first_ns.view(np.uint32), b.first_ns.view(np.uint32))
+    assert a.counters() == b.counters()
+
+
+# ---- RNG ----------------------------------------------------------------------------
+def test_philox_matches_oracle_and_curand(engine, oracle):
+    rng = np.random.default_rng(1)
+    ctr = rng.integers(0, 2 ** 32, size=(100_000, 4), dtype=np.uint64).astype(np.uint32)
+    seed = 0x9E3779B97F4A7C15
+    dev = engine.philox(ctr, seed)
+    assert np.array_equal(dev, oracle.philox_batch(ctr, seed))
+    assert np.array_equal(dev, engine.philox(ctr, seed, use_curand=True))
+
+
+def test_randu_streams_match_oracle(engine, oracle):
+    for seed in (1, 1234, 2 ** 40 + 7):
+        dev = engine.randu_streams(seed, 20_000, 37)
+        ref = oracle.randu_streams(seed, 20_000, 37)
+        assert np.array_equal(dev.view(np.uint32), ref.view(np.uint32))
+
+
+# ---- elementary functions ------------------------------------------------------------
+ALL_RANDU = ((np.arange(2 ** 24, dtype=np.float32) + np.float32(1)) * np.float32(2.0 ** -24))
+
+
+def test_log_exhaustive_over_uniforms(engine, oracle):
+    """Every argument the transport passes to log is a uniform ((x>>8)+1)2^-24:
+    all 2^24 of them give the oracle's bits."""
+    dev = engine.eval_math("log", ALL_RANDU)
+    ref = oracle.eval_math("log", ALL_RANDU)
+    bad = np.flatnonzero(dev.view(np.uint32) != ref.view(np.uint32))
+    print("log mismatches:", bad.size)
+    assert bad.size == 0
+
+
+def test_sincos_exhaustive_over_azimuths(engine, oracle):
+    """All 2^24 azimuths (2f0*Float32(pi))*u."""
+    phi = (np.float32(2.0) * np.float32(math.pi)) * ALL_RANDU
+    for fn in ("sin", "cos"):
+        dev = engine.eval_math(fn, phi)
+        ref = oracle.eval_math(fn, phi)
+        bad = np.flatnonzero(dev.view(np.uint32) != ref.view(np.uint32))
+        print(fn, "mismatches:", bad.size)
+        assert bad.size == 0
+
+
+def test_sincos_facet_angles(engine, oracle):
+    """Facet tilts alpha in [0, 1.2): every Float32 in a dense sample."""
+    rng = np.random.default_rng(5)
+    a = np.concatenate([rng.uniform(0, 1.2, 8_000_000).astype(np.float32),
+                        np.linspace(0, 1.2, 1_000_001, dtype=np.float32),
+                        np.float32([0.0, 1e-30, 1e-7, np.pi / 4, np.pi / 2, 1.19999])])
+    for fn in ("sin", "cos"):
+        dev = engine.eval_math(fn, a)
+        ref = oracle.eval_math(fn, a)
+        nbad = int((dev.view(np.uint32) != ref.view(np.uint32)).sum())
+        print(fn, "mismatches:", nbad, "of", a.size)
+        assert nbad <= a.size * 1e-6
+
+
+def test_math_special_values(engine, oracle):
+    x = np.float32([1.0, 2.0 ** -24, 0.5, 2.0, 1e-40, 0.0, np.inf, 3e38, 1.4142135,
+                    1.4142137, 0.70710677])
+    with np.errstate(all="ignore"):
+        dev = engine.eval_math("log", x)
+        ref = oracle.eval_math("log", x)
+        assert np.array_equal(dev.view(np.uint32), ref.view(np.uint32))
+        assert np.isnan(engine.eval_math("log", np.float32([-1.0, np.nan]))).all()
+    y = np.float32([0.0, -0.0, 1e4, -1e4, 1e5, 123456.7, -3.0, 1e-20])
+    for fn in ("sin", "cos"):
+        assert np.array_equal(engine.eval_math(fn, y).view(np.uint32),
+                              oracle.eval_math(fn, y).view(np.uint32))
+
+
+# ---- transport: per-photon records ------------------------------------------------------
+CASES = {
+    # name: (box, op, readout, tb, kwargs)
+    "config1_csitl_teflon": (BOX_CSI, OP_C1, Readout(GRID), TB80,
+                             dict(n_photons=200_000, seed=1234, pos=CENTRE_CSI, tau_ns=TAU_C1)),
+    "config2_bgo_esr_centre": (BOX_BGO, OP_C2, Readout(GRID), TB80,
+                               dict(n_photons=100_000, seed=1234, pos=CENTRE_BGO, tau_ns=TAU_C2)),
+    "all_processes_disc_surround": (BOX_CSI, OP_ALL, RO_ALL, TB,
+                                    dict(n_photons=100_000, seed=8, pos=CENTRE_CSI, tau_ns=800.0)),
+    "all_processes_two_sided": (BOX_CSI, OP_ALL, Readout(GRID, two_sided=True), TB,
+                                dict(n_photons=100_000, seed=8, pos=CENTRE_CSI, tau_ns=800.0)),
+    "front_painted_lambertian": (BOX_CSI, ideal(1.79, wrap_R=0.95, gap=False, abs_len=3000.0),
+                                 Readout(GRID), TB, dict(n_photons=50_000, seed=7, pos=CENTRE_CSI,
+                                                         tau_ns=0.0)),
+    "front_painted_specular": (BOX_BGO, ideal(2.15, wrap_R=0.97, gap=False, spec=True,
+                                              abs_len=2000.0), Readout(GRID), TB,
+                               dict(n_photons=50_000, seed=9, pos=CENTRE_BGO, tau_ns=0.0)),
+    "polished_backpainted": (BOX_CSI, ideal(1.95, wrap_R=0.98, abs_len=800.0, ray=500.0, pde=0.7),
+                             Readout(GRID, center=(20, 26), radius=15, sur_R=0.8,
+                                     sur_specular=True), TB,
+                             dict(n_photons=50_000, seed=10, pos=(10.0, 30.0, 5.0), tau_ns=300.0)),
+    "bench_cold_csi_delta": (BOX_CSI, OP_BENCH, Readout(GRID), TB80,
+                             dict(n_photons=100_000, seed=1, pos=CENTRE_CSI, tau_ns=0.0)),
+    "scan_round_robin_t0_offset": (BOX_CSI, OP_ALL, RO_ALL, TB,
+                                   dict(n_photons=60_001, seed=23,
+                                        positions=[(24.0, 24.0, 5.0), (24.0, 24.0, 30.0),
+                                                   (3.0, 40.0, 1.0)],
+                                        t0s=[0.0, 55.5, 7000.0], pid_offset=123_456_789,
+                                        tau_ns=800.0)),
+    "cap_and_overflow": (BOX_CSI, ideal(1.95), Readout(GRID), TimeBinning(1.0, 3),
+                         dict(n_photons=20_000, seed=2, pos=CENTRE_CSI, tau_ns=0.0,
+                              max_bounces=50)),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_transport_matches_oracle(engine, oracle, name):
+    box, op, ro, tb, kw = CASES[name]
+    dacc, drec = engine.run_photons_ka(box, op, ro, tb, return_records=True, **kw)
+    (oacc, orec), steps = oracle.run_photons_ka(box, op, ro, tb, return_records=True,
+                                                nthreads=NT, return_steps=True, **kw)
+    nonexact = _assert_records_equal(drec, orec)
+    assert dacc.total_terminated() == kw["n_photons"]
+    assert dacc.counts.sum() == dacc.ndet
+    assert engine.last_steps == steps or nonexact > 0
+    if nonexact == 0:
+        _assert_acc_equal(dacc, oacc)
+
+
+def test_accumulator_without_records_matches(engine, oracle):
+    """The tile path (no records) produces the same Accumulator as the oracle's
+    threaded run_photons! (src/transport.jl:245-273)."""
+    box, op, ro, tb, kw = CASES["config1_csitl_teflon"]
+    dacc = engine.run_photons(box, op, ro, tb, n_photons=kw["n_photons"], seed=kw["seed"],
+                              pos=kw["pos"], tau_ns=kw["tau_ns"])
+    oacc = oracle.run_photons(box, op, ro, tb, n_photons=kw["n_photons"], seed=kw["seed"],
+                              pos=kw["pos"], tau_ns=kw["tau_ns"], nthreads=NT)
+    _assert_acc_equal(dacc, oacc)
+
+
+def test_launch_shape_does_not_change_results(engine):
+    box, op, ro, tb, kw = CASES["all_processes_disc_surround"]
+    ref = engine.run_photons_ka(box, op, ro, tb, **kw)
+    try:
+        for shape in ((1, 64, 32), (2, 128, 256), (0, 256, 4096)):
+            engine.set_launch(*shape)
+            _assert_acc_equal(engine.run_photons_ka(box, op, ro, tb, **kw), ref)
+    finally:
+        engine.set_launch(0, 0, 0)
+
+
+def test_global_tile_path_for_long_histograms(engine, oracle):
+    """A histogram too large for shared memory takes the global-atomics path."""
+    tb = TimeBinning(0.5, 60_000)      # 64 x 60001 bins > shared memory
+    kw = dict(n_photons=30_000, seed=77, pos=CENTRE_CSI, tau_ns=1000.0)
+    d = engine.run_photons_ka(BOX_CSI, OP_C1, Readout(GRID), tb, **kw)
+    o = oracle.run_photons_ka(BOX_CSI, OP_C1, Readout(GRID), tb, nthreads=NT, **kw)
+    _assert_acc_equal(d, o)
+
+
+def test_empty_and_single_photon(engine, oracle):
+    acc = engine.run_photons_ka(BOX_CSI, OP_C1, GRID, TB, n_photons=0, seed=1, pos=CENTRE_CSI,
+                                tau_ns=1000.0)
+    assert acc.counts.sum() == 0 and np.all(np.isinf(acc.first_ns)) and acc.total_terminated() == 0
+    for seed in (1, 2, 3):
+        d, dr = engine.run_photons_ka(BOX_CSI, OP_C1, GRID, TB, n_photons=1, seed=seed,
+                                      pos=CENTRE_CSI, tau_ns=1000.0, return_records=True)
+        o, orr = oracle.run_photons_ka(BOX_CSI, OP_C1, GRID, TB, n_photons=1, seed=seed,
+                                       pos=CENTRE_CSI, tau_ns=1000.0, return_records=True)
+        _assert_acc_equal(d, o)
+        assert dr.status[0] == orr.status[0] and dr.t[0] == orr.t[0]
+
+
+def test_bad_arguments_are_rejected(engine):
+    from crysplight_b200._lib import CudaTransportError
+    with pytest.raises(CudaTransportError):
+        engine.run_photons_ka(Box((48, 48, -1)), OP_C1, GRID, TB, n_photons=10, seed=1,
+                              pos=CENTRE_CSI, tau_ns=0.0)
+    with pytest.raises(CudaTransportError):
+        engine.run_photons_ka(BOX_CSI, OP_C1, SipmGrid(6, 300, 300), TB, n_photons=10, seed=1,
+                              pos=CENTRE_CSI, tau_ns=0.0)
+    with pytest.raises(CudaTransportError):
+        engine.run_photons_ka(BOX_CSI, OP_C1, GRID, TimeBinning(0.0, 10), n_photons=10, seed=1,
+                              pos=CENTRE_CSI, tau_ns=0.0)
+    # the handle is still usable afterwards
+    acc = engine.run_photons_ka(BOX_CSI, OP_C1, GRID, TB, n_photons=1000, seed=1,
+                                pos=CENTRE_CSI, tau_ns=0.0)
+    assert acc.total_terminated() == 1000
+
+
+# ---- segments (scan points / events) ----------------------------------------------------
+def _segment_case(rng, n_src=300, n_seg=40):
+    src = np.column_stack([rng.uniform(0, 48, n_src), rng.uniform(0, 48, n_src),
+                           rng.uniform(0, 37.2, n_src)]).astype(np.float32)
+    counts = rng.integers(0, 700, n_src)
+    counts[rng.random(n_src) < 0.2] = 0                     # empty sources
+    seg = np.sort(rng.integers(0, n_seg, n_src)).astype(np.int32)
+    t0 = rng.uniform(0, 0.5, n_src).astype(np.float32)
+    return src, counts, seg, t0
+
+
+def test_segments_match_oracle(engine, oracle):
+    rng = np.random.default_rng(11)
+    src, counts, seg, t0 = _segment_case(rng)
+    kw = dict(sources=src, photons_per_source=counts, segment_of_source=seg, n_segments=40,
+              seed=11, t0s=t0, pid_offset=1000, tau_ns=1000.0)
+    dres, drec = engine.run_segments(BOX_CSI, OP_C1, GRID, TB80, return_records=True, **kw)
+    ores, orec = oracle.run_segments(BOX_CSI, OP_C1, GRID, TB80, return_records=True,
+                                     nthreads=NT, **kw)
+    nonexact = _assert_records_equal(drec, orec)
+    assert dres.counters["ndet"] == int(dres.npe.sum())
+    assert np.array_equal(dres.maps.sum(axis=(0, 1)), dres.npe)
+    assert np.array_equal(np.isfinite(dres.tmin), dres.maps > 0)
+    if nonexact == 0:
+        assert np.array_equal(dres.maps, ores["maps"])
+        assert np.array_equal(dres.tmin.view(np.uint32), ores["tmin"].view(np.uint32))
+        assert np.array_equal(dres.npe, ores["npe"])
+        assert dres.counters == ores["counters"]
+
+
+def test_segments_equal_point_runs(engine):
+    """A scan as segments gives, point by point, what one run_photons_ka! call
+    per point with pid_offset = photons before it gives."""
+    pts = scan_points(5, BOX_BGO, seed=7)
+    per = 20_000
+    res = engine.run_segments(BOX_BGO, OP_C2, GRID, TB80, sources=pts,
+                              photons_per_source=[per] * 5, segment_of_source=range(5),
+                              n_segments=5, seed=1234, tau_ns=TAU_C2)
+    for p in range(5):
+        acc = engine.run_photons_ka(BOX_BGO, OP_C2, GRID, TB80, n_photons=per, seed=1234,
+                                    pos=tuple(pts[p]), pid_offset=p * per, tau_ns=TAU_C2)
+        assert np.array_equal(acc.counts.sum(axis=2), res.maps[:, :, p])
+        assert np.array_equal(acc.first_ns.view(np.uint32), res.tmin[:, :, p].view(np.uint32))
+        assert acc.ndet == res.npe[p]
+
+
+# ---- full BASELINE sizes: exact where the oracle is fast, properties otherwise -----------
+def test_config1_full_size_exact(engine, oracle):
+    """Config 1 at its full 1,000,000 photons: identical to the oracle."""
+    kw = dict(n_photons=1_000_000, seed=1234, pos=CENTRE_CSI, tau_ns=TAU_C1)
+    d = engine.run_photons(BOX_CSI, OP_C1, GRID, TB80, **kw)
+    o = oracle.run_photons(BOX_CSI, OP_C1, GRID, TB80, nthreads=NT, **kw)
+    _assert_acc_equal(d, o)
+    assert abs(d.ndet / 1e6 - 0.888) < 0.002
+
+
+def test_config2_full_size_properties(engine, oracle):
+    """Config 2 at full size: 256 points x 200,000 photons (51.2M).  Size-
+    independent properties on the whole run; exact equality on 4 points."""
+    pts = scan_points(256, BOX_BGO, seed=7)
+    per = 200_000
+    res = engine.run_segments(BOX_BGO, OP_C2, GRID, TB80, sources=pts,
+                              photons_per_source=[per] * 256, segment_of_source=range(256),
+                              n_segments=256, seed=1234, tau_ns=TAU_C2)
+    c = res.counters
+    assert sum(c[k] for k in ("ndet", "nabs_bulk", "nabs_wall", "nabs_sipm", "ncap",
+                              "nabs_sur")) == 256 * per
+    assert int(res.npe.sum()) == c["ndet"]
+    assert np.array_equal(res.maps.sum(axis=(0, 1)), res.npe)
+    assert np.array_equal(np.isfinite(res.tmin), res.maps > 0)
+    frac = res.npe / per
+    assert 0.3 < frac.min() and frac.max() < 0.95
+    for p in (0, 17, 128, 255):
+        sub = oracle.run_segments(BOX_BGO, OP_C2, GRID, TB80, sources=pts[p:p + 1],
+                                  photons_per_source=[per], segment_of_source=[0], n_segments=1,
+                                  seed=1234, pid_offset=p * per, tau_ns=TAU_C2, nthreads=NT)
+        assert np.array_equal(sub["maps"][:, :, 0], res.maps[:, :, p])
+        assert np.array_equal(sub["tmin"][:, :, 0].view(np.uint32),
+                              res.tmin[:, :, p].view(np.uint32))
