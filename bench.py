@@ -202,7 +202,8 @@ def run_cuda_arm(args, W, rank, world, local_rank):
         import torch.distributed as dist
 
     pid_base = rank * W["n"]        # disjoint photon ids per rank
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # explicit stream: the library launches on it
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
     nx = ny = 8
     pts = W["points"]

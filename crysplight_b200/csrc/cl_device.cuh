@@ -150,6 +150,11 @@ __device__ __forceinline__ void cl_sincosf(float x, float* sp, float* cp)
         *cp = __double2float_rn(cos(xd));
         return;
     }
+    if (xd == 0.0) {                           // sin(+-0) = +-0, cos(+-0) = 1
+        *sp = x;
+        *cp = 1.0f;
+        return;
+    }
     const double q = rint(xd * CLM_2_OVER_PI);
     double r = fma(-q, CLM_PIO2_HI, xd);
     r = fma(-q, CLM_PIO2_LO, r);

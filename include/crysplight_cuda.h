@@ -167,8 +167,9 @@ int cl_run_photons(cl_handle* h,
 
 /*
  * Same as cl_run_photons with every pointer in device memory, enqueued on
- * `stream` (a cudaStream_t; NULL = the handle's own stream) without a host
- * synchronisation.  `counters` is device memory too.  Call cl_sync() to wait
+ * `stream` (a cudaStream_t; NULL = the handle's own stream, so pass
+ * cudaStreamLegacy or cudaStreamPerThread to select a default stream) without
+ * a host synchronisation.  `counters` is device memory too.  Call cl_sync() to wait
  * and to collect device-side errors.
  */
 int cl_run_photons_device(cl_handle* h,
