@@ -20,7 +20,7 @@ EXPORTS = (
     "cl_version", "cl_abi_version", "cl_create", "cl_destroy", "cl_last_error",
     "cl_run_photons", "cl_run_photons_device", "cl_run_segments",
     "cl_run_segments_device", "cl_sync", "cl_last_steps", "cl_set_launch",
-    "cl_debug_eval",
+    "cl_debug_eval", "cl_run_photons_noalloc",
 )
 
 CL_OK = 0
@@ -83,6 +83,10 @@ def _declare(lib: C.CDLL) -> None:
     lib.cl_set_launch.restype = C.c_int
     lib.cl_debug_eval.argtypes = [_P, C.c_int, _P, _P, C.c_int64, C.c_uint64, C.c_int32]
     lib.cl_debug_eval.restype = C.c_int
+    lib.cl_run_photons_noalloc.argtypes = common[1:] + [
+        _P, _P, _P, _P, C.c_int32, C.c_int64, C.c_uint64, C.c_uint64, C.c_float, C.c_int32,
+        _P, _P, C.POINTER(Counters), _P]
+    lib.cl_run_photons_noalloc.restype = C.c_int
 
 
 def load() -> C.CDLL:

@@ -22,6 +22,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
+#include <mutex>
 #include <new>
 
 #include <cuda_runtime.h>
@@ -973,3 +974,142 @@ int cl_debug_eval(cl_handle* h, int fn, const void* in, void* out, int64_t n, ui
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free entry point (cl_run_photons_noalloc).
+//
+// For callers that cannot let a library call cudaMalloc (device memory owned
+// by a pool/caching allocator or a fixed budget; loops where cudaMalloc or
+// cudaFree would synchronise the device).  All device memory it touches is
+// the file-scope array below, CL_NOALLOC_SCRATCH_BYTES long, which each GPU
+// that loads this library holds until the process exits.  Every call reuses
+// (and overwrites) the whole array: calls that overlap on the GPU race.
+// ===========================================================================
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CL_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+struct NoallocDevice {
+    bool ready = false;
+    unsigned char* base = nullptr;   // device address of g_noalloc_scratch on this device
+    int num_sms = 0;
+    int max_smem_optin = 0;
+};
+NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
+
+// Once per device, with that device current: look up the array's device
+// address (host code cannot use the symbol itself as a device pointer) and
+// the launch limits.  Allocates nothing.
+int noalloc_setup(int dev, NoallocDevice** out)
+{
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoallocDevice& d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess)
+            e = cudaDeviceGetAttribute(&d.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            snprintf(g_create_err, sizeof g_create_err, "cl_run_photons_noalloc: set-up on device %d: %s",
+                     dev, cudaGetErrorString(e));
+            return CL_ERR_CUDA;
+        }
+        set_kernel_attrs<0, false, true>(d.max_smem_optin);
+        set_kernel_attrs<0, false, false>(d.max_smem_optin);
+        cudaGetLastError();
+        d.base = (unsigned char*)p;
+        d.ready = true;
+    }
+    *out = &d;
+    return CL_OK;
+}
+}  // namespace
+
+extern "C" int cl_run_photons_noalloc(const cl_box* box, const cl_optical_params* op,
+                                      const cl_readout* ro, const cl_time_binning* tb,
+                                      const float* px, const float* py, const float* pz,
+                                      const float* pt, int32_t npos,
+                                      int64_t n_photons, uint64_t seed, uint64_t pid_offset,
+                                      float tau_ns, int32_t max_bounces,
+                                      uint32_t* counts, float* first_ns, cl_counters* counters,
+                                      void* stream)
+{
+    g_create_err[0] = 0;
+    // A stack handle carries the launch settings and collects error messages;
+    // its scratch words point into the static array.  Nothing is allocated.
+    cl_handle tmp;
+    auto fail = [&](int rc) {
+        snprintf(g_create_err, sizeof g_create_err, "cl_run_photons_noalloc: %s", tmp.err);
+        return rc;
+    };
+    int rc = check_params(&tmp, box, op, ro, tb, tau_ns);
+    if (rc != CL_OK) return fail(rc);
+    if (npos < 1 || !px || !py || !pz) return fail(set_err(&tmp, CL_ERR_ARG, "need npos >= 1 source positions"));
+    if (n_photons < 0) return fail(set_err(&tmp, CL_ERR_ARG, "n_photons must be >= 0"));
+    if (!counts || !first_ns || !counters) return fail(set_err(&tmp, CL_ERR_ARG, "null output buffer"));
+
+    const int cells = ro->grid.nx * ro->grid.ny;
+    const size_t n_counts = (size_t)cells * (size_t)(tb->nbins + 1);
+    const size_t b_words = 256, b_ctr = 256;
+    const size_t b_counts = align256(n_counts * sizeof(uint32_t));
+    const size_t b_keys = align256((size_t)cells * sizeof(uint32_t));
+    const size_t b_src = align256((size_t)npos * sizeof(float));
+    const size_t need = b_words + b_ctr + b_counts + b_keys + 4 * b_src;
+    if (need > (size_t)CL_NOALLOC_SCRATCH_BYTES)
+        return fail(set_err(&tmp, CL_ERR_ARG,
+                            "staged data needs %zu bytes (npos %d, %d cells x %d bins) but the "
+                            "static device array holds %u bytes",
+                            need, (int)npos, cells, tb->nbins + 1, (unsigned)CL_NOALLOC_SCRATCH_BYTES));
+
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        cudaGetLastError();
+        return fail(set_err(&tmp, CL_ERR_CUDA, "no current CUDA device (%s)",
+                            e != cudaSuccess ? cudaGetErrorString(e) : "device index out of range"));
+    }
+    NoallocDevice* nd = nullptr;
+    if ((rc = noalloc_setup(dev, &nd)) != CL_OK) return rc;
+
+    tmp.device = dev;
+    tmp.num_sms = nd->num_sms;
+    tmp.max_smem_optin = nd->max_smem_optin;
+    tmp.scratch.p = nd->base;                 // queue / steps / done / err words
+    tmp.scratch.cap = b_words;
+    unsigned char* base = nd->base;
+    unsigned long long* d_ctr = (unsigned long long*)(base + b_words);
+    uint32_t* d_counts = (uint32_t*)(base + b_words + b_ctr);
+    uint32_t* d_keys = (uint32_t*)(base + b_words + b_ctr + b_counts);
+    float* d_px = (float*)(base + b_words + b_ctr + b_counts + b_keys);
+    float* d_py = (float*)((unsigned char*)d_px + b_src);
+    float* d_pz = (float*)((unsigned char*)d_py + b_src);
+    float* d_pt = (float*)((unsigned char*)d_pz + b_src);
+    cudaStream_t st = (cudaStream_t)stream;
+
+#define NK(call, what)                                                        \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return fail(cuda_fail(&tmp, e_, (what)));      \
+    } while (0)
+    NK(cudaMemcpyAsync(d_px, px, npos * sizeof(float), cudaMemcpyHostToDevice, st), "copy px");
+    NK(cudaMemcpyAsync(d_py, py, npos * sizeof(float), cudaMemcpyHostToDevice, st), "copy py");
+    NK(cudaMemcpyAsync(d_pz, pz, npos * sizeof(float), cudaMemcpyHostToDevice, st), "copy pz");
+    if (pt) NK(cudaMemcpyAsync(d_pt, pt, npos * sizeof(float), cudaMemcpyHostToDevice, st), "copy pt");
+
+    // The init kernel clears the counts, keys, counters and queue words left
+    // by the previous call before the transport kernel runs.
+    const Physics P = make_physics(box, op, ro, tb, tau_ns, max_bounces, seed);
+    rc = enqueue_point(&tmp, P, d_px, d_py, d_pz, pt ? d_pt : nullptr, npos, n_photons, pid_offset,
+                       d_counts, d_keys, d_ctr, nullptr, st);
+    if (rc != CL_OK) return fail(rc);
+    NK(cudaMemcpyAsync(counts, d_counts, n_counts * sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "copy counts");
+    NK(cudaMemcpyAsync(first_ns, d_keys, (size_t)cells * sizeof(float), cudaMemcpyDeviceToHost, st), "copy first_ns");
+    NK(cudaMemcpyAsync(counters, d_ctr, sizeof(cl_counters), cudaMemcpyDeviceToHost, st), "copy counters");
+#undef NK
+    rc = collect(&tmp, st);
+    if (rc != CL_OK) return fail(rc);
+    return CL_OK;
+}

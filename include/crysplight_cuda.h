@@ -136,7 +136,8 @@ int cl_abi_version(void);
 int cl_create(cl_handle** out, int device);
 void cl_destroy(cl_handle* h);
 /* Message of the last failing call on this handle ("" if none).  With a NULL
- * handle, the message of the last failing cl_create on this thread. */
+ * handle, the message of the last failing cl_create or cl_run_photons_noalloc
+ * on this thread. */
 const char* cl_last_error(const cl_handle* h);
 
 /*
@@ -260,6 +261,44 @@ int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta,
  */
 int cl_debug_eval(cl_handle* h, int fn, const void* in, void* out, int64_t n,
                   uint64_t seed, int32_t n_per);
+
+/*
+ * Allocation-free point-source transport.  No counterpart in the reference:
+ * it exists for callers that cannot let a library call cudaMalloc — programs
+ * whose device memory is owned by a pool or caching allocator (CUDA.jl's,
+ * PyTorch's) or by a fixed budget, where a foreign cudaMalloc can fail or
+ * break the accounting, and latency-sensitive loops where cudaMalloc/cudaFree
+ * would synchronise the device.
+ *
+ * Same arguments and results as cl_run_photons with host buffers, minus the
+ * handle and the per-photon records.  All device-side memory it uses —
+ * staged source positions, the count histogram, first-time keys, counters and
+ * the work-queue words — lives in one file-scope device array of
+ * CL_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * process exit.  The staged data is 512 bytes of queue words and counters
+ * plus four float arrays of npos, nx*ny*(nbins+1) count words and nx*ny key
+ * words, each array rounded up to a multiple of 256 bytes; calls where that
+ * exceeds CL_NOALLOC_SCRATCH_BYTES (1 MiB: e.g. an 8x8 grid with up to about
+ * 4000 time bins) return CL_ERR_ARG with a message from cl_last_error(NULL).
+ * The function calls no cudaMalloc, cudaFree or allocating library routine.
+ *
+ * Runs on the current CUDA device and on `stream` (NULL = the legacy default
+ * stream), and synchronises that stream before returning.  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress) and
+ * caches it; make that first call before any stream capture.  Every call
+ * shares the one array and overwrites it, so calls that overlap on the GPU
+ * (other host threads, other streams) race: serialise them.
+ */
+#define CL_NOALLOC_SCRATCH_BYTES (1u << 20)
+
+int cl_run_photons_noalloc(const cl_box* box, const cl_optical_params* op,
+                           const cl_readout* ro, const cl_time_binning* tb,
+                           const float* px, const float* py, const float* pz,
+                           const float* pt, int32_t npos,
+                           int64_t n_photons, uint64_t seed, uint64_t pid_offset,
+                           float tau_ns, int32_t max_bounces,
+                           uint32_t* counts, float* first_ns, cl_counters* counters,
+                           void* stream);
 
 #ifdef __cplusplus
 }
