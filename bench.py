@@ -44,7 +44,7 @@ OPS_PER_STEP = {"scan256": 165.6, "point1m": 186.7}
 L2_FLUSH_BYTES = 256 << 20
 
 
-def workload(name: str):
+def workload(name: str, points: int = 256, per_point: int = 200_000):
     from crysplight_b200.params import (Box, OpticalParams, Readout, SipmGrid, TimeBinning,
                                         deg2rad_f32)
     from crysplight_b200.scan import scan_points
@@ -52,10 +52,11 @@ def workload(name: str):
     if name == "scan256":
         box = Box((48.0, 48.0, 22.4))
         op = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, deg2rad_f32(1.3), 1.0)
-        pts = scan_points(256, box, seed=7)
+        pts = scan_points(256, box, seed=7)[:points]
         return dict(name=name, box=box, op=op, ro=Readout(grid), tb=tb, tau=1768.0, seed=1234,
-                    points=pts, per_point=200_000, n=256 * 200_000,
-                    desc="BGO+ESR 48x48x22.4 mm, 256 points x 200000 photons, per-point 8x8 maps")
+                    points=pts, per_point=per_point, n=points * per_point,
+                    desc=f"BGO+ESR 48x48x22.4 mm, {points} points x {per_point} photons, "
+                         "per-point 8x8 maps")
     box = Box((48.0, 48.0, 37.2))
     op = OpticalParams(1.79, 1.45, 3115.0, 346.0, 0.99, False, True, deg2rad_f32(1.3), 1.0)
     return dict(name=name, box=box, op=op, ro=Readout(grid), tb=tb, tau=1000.0, seed=1234,
@@ -370,13 +371,16 @@ def main():
     ap.add_argument("--workload", choices=("scan256", "point1m"), default="scan256")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--points", type=int, default=256,
+                    help="scan256: use only the first N points (profiling of a smaller case)")
+    ap.add_argument("--photons-per-point", type=int, default=200_000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    W = workload(args.workload)
+    W = workload(args.workload, args.points, args.photons_per_point)
     if args.impl == "reference":
         run_reference_arm(args, W, rank, world)
         return

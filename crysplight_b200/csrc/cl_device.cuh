@@ -1,6 +1,6 @@
 // cl_device.cuh — device-side building blocks of the transport engine:
 // Philox4x32-10 streams, Float32 elementary functions, and the per-photon
-// physics of one bounce-loop iteration.
+// physics primitives the transport kernel's state machine composes.
 //
 // Arithmetic contract (what makes results identical to the reference's CPU
 // transport, src/transport.jl):
@@ -42,64 +42,82 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
     return c;
 }
 
-// A photon's uniform stream (PhiloxStream / PhiloxState, src/philox.jl:34-62,
-// src/kernel.jl:15-46).  Key = seed, counter = (pid lo, pid hi, block, 0).
-// Up to eight outputs (two blocks) are buffered; draw() pops in order, so the
-// sequence is the reference's regardless of when blocks are generated.
-struct Stream {
+// randu, src/philox.jl:62: ((x >>> 8) + 1.0f0) * 2^-24, exact, in (0, 1].
+__device__ __forceinline__ float u32_to_randu(uint32_t x)
+{
+    return __fmul_rn(__fadd_rn((float)(x >> 8), 1.0f), 0x1p-24f);
+}
+
+// A photon's uniform stream (PhiloxStream, src/philox.jl:34-62): key = seed,
+// counter = (pid lo, pid hi, block, 0).  The outputs are buffered in a
+// per-lane ring of RING_LEN words in shared memory (word i of lane `tid` at
+// ring[(i % RING_LEN) * blockDim + tid]: every access is bank-conflict free).
+// Blocks are generated ahead of use, at one convergent point of the warp
+// loop; pop() consumes in order and peek(d) looks d words ahead, so the
+// sequence of uniforms is exactly the reference's.
+constexpr int RING_LEN = 16;
+
+struct Rng {
     uint32_t pid_lo, pid_hi, block;
-    uint32_t b0, b1, b2, b3, b4, b5, b6, b7;
-    int n;  // buffered outputs
+    uint32_t head;   // index of the next unread word
+    int cnt;         // buffered words
 };
 
-__device__ __forceinline__ void stream_init(Stream& s, uint64_t pid)
+__device__ __forceinline__ void rng_init(Rng& r, uint64_t pid)
 {
-    s.pid_lo = (uint32_t)pid;
-    s.pid_hi = (uint32_t)(pid >> 32);
-    s.block = 0;
-    s.n = 0;
-    s.b0 = s.b1 = s.b2 = s.b3 = s.b4 = s.b5 = s.b6 = s.b7 = 0;
+    r.pid_lo = (uint32_t)pid;
+    r.pid_hi = (uint32_t)(pid >> 32);
+    r.block = 0;
+    r.head = 0;
+    r.cnt = 0;
 }
 
-// Append one block behind the buffered outputs (requires n <= 4).
-__device__ __forceinline__ void stream_fill(Stream& s, uint32_t k0, uint32_t k1)
+__device__ __forceinline__ void rng_fill(Rng& r, uint32_t* ring, int stride, uint32_t k0, uint32_t k1)
 {
-    const uint4 o = philox4x32_10(make_uint4(s.pid_lo, s.pid_hi, s.block, 0u), k0, k1);
-    s.block += 1u;
+    const uint4 o = philox4x32_10(make_uint4(r.pid_lo, r.pid_hi, r.block, 0u), k0, k1);
+    r.block += 1u;
+    const uint32_t w = r.head + (uint32_t)r.cnt;
+    ring[((w + 0u) % RING_LEN) * stride] = o.x;
+    ring[((w + 1u) % RING_LEN) * stride] = o.y;
+    ring[((w + 2u) % RING_LEN) * stride] = o.z;
+    ring[((w + 3u) % RING_LEN) * stride] = o.w;
+    r.cnt += 4;
+}
+
+__device__ __forceinline__ float rng_peek(const Rng& r, const uint32_t* ring, int stride, uint32_t d)
+{
+    return u32_to_randu(ring[((r.head + d) % RING_LEN) * stride]);
+}
+
+// Pop the next uniform.  The warp loop keeps at least as many words buffered
+// as one iteration can consume; `under` records a violation of that bound.
+__device__ __forceinline__ float rng_pop(Rng& r, const uint32_t* ring, int stride, bool& under)
+{
+    under |= r.cnt <= 0;
+    const float u = u32_to_randu(ring[(r.head % RING_LEN) * stride]);
+    r.head += 1u;
+    r.cnt -= 1;
+    return u;
+}
+
+// A register-only stream for the diagnostics kernel (same sequence).
+struct SimpleStream {
+    uint32_t pid_lo, pid_hi, block, b0, b1, b2, b3;
+    int n;
+};
+
+__device__ __forceinline__ float simple_randu(SimpleStream& s, uint32_t k0, uint32_t k1)
+{
     if (s.n == 0) {
+        const uint4 o = philox4x32_10(make_uint4(s.pid_lo, s.pid_hi, s.block, 0u), k0, k1);
+        s.block += 1u;
         s.b0 = o.x; s.b1 = o.y; s.b2 = o.z; s.b3 = o.w;
-    } else {
-        // n in 1..4: place after the n buffered outputs
-        if (s.n == 1) { s.b1 = o.x; s.b2 = o.y; s.b3 = o.z; s.b4 = o.w; }
-        else if (s.n == 2) { s.b2 = o.x; s.b3 = o.y; s.b4 = o.z; s.b5 = o.w; }
-        else if (s.n == 3) { s.b3 = o.x; s.b4 = o.y; s.b5 = o.z; s.b6 = o.w; }
-        else { s.b4 = o.x; s.b5 = o.y; s.b6 = o.z; s.b7 = o.w; }
+        s.n = 4;
     }
-    s.n += 4;
-}
-
-// Top the buffer up to at least 5 outputs; called at convergent points so
-// the Philox rounds execute once for the whole warp.
-__device__ __forceinline__ void stream_topup(Stream& s, uint32_t k0, uint32_t k1)
-{
-    if (s.n <= 4) stream_fill(s, k0, k1);
-}
-
-__device__ __forceinline__ uint32_t stream_next(Stream& s, uint32_t k0, uint32_t k1)
-{
-    if (s.n == 0) stream_fill(s, k0, k1);
     const uint32_t x = s.b0;
-    s.b0 = s.b1; s.b1 = s.b2; s.b2 = s.b3; s.b3 = s.b4;
-    s.b4 = s.b5; s.b5 = s.b6; s.b6 = s.b7;
+    s.b0 = s.b1; s.b1 = s.b2; s.b2 = s.b3;
     s.n -= 1;
-    return x;
-}
-
-// randu, src/philox.jl:62: ((x >>> 8) + 1.0f0) * 2^-24, exact, in (0, 1].
-__device__ __forceinline__ float randu(Stream& s, uint32_t k0, uint32_t k1)
-{
-    const uint32_t x = stream_next(s, k0, k1);
-    return __fmul_rn(__fadd_rn((float)(x >> 8), 1.0f), 0x1p-24f);
+    return u32_to_randu(x);
 }
 
 // ---------------------------------------------------------------------------
@@ -110,6 +128,15 @@ __device__ __forceinline__ float randu(Stream& s, uint32_t k0, uint32_t k1)
 // through the CUDA double-precision library functions.
 // ---------------------------------------------------------------------------
 
+// Out-of-domain arguments (never reached by the transport): CUDA's Float64
+// functions, kept out of line so the hot loop stays small.
+__device__ __noinline__ float slow_logf(float x) { return __double2float_rn(log((double)x)); }
+__device__ __noinline__ float2 slow_sincosf(float x)
+{
+    const double xd = (double)x;
+    return make_float2(__double2float_rn(sin(xd)), __double2float_rn(cos(xd)));
+}
+
 // Natural log.  Table-driven (Tang 1990): x = 2^e * m, m in [sqrt(1/2), sqrt(2)),
 // m = F_j (1 + r) with F_j = 1 + j/64, ln x = e ln2 + ln F_j + log1p(r),
 // |r| < 1/90, log1p by its Taylor series to r^8.
@@ -117,7 +144,7 @@ __device__ __forceinline__ float cl_logf(float x, const double2* __restrict__ ta
 {
     const uint32_t b = __float_as_uint(x);
     if (b - 0x00800000u >= 0x7f000000u)       // not a positive normal finite float
-        return __double2float_rn(log((double)x));
+        return slow_logf(x);
     int e = (int)(b >> 23) - 127;
     uint32_t mb = b & 0x007fffffu;
     const int hi = mb >= 0x3504f3u;          // m >= sqrt(2): use m/2, e+1
@@ -146,8 +173,9 @@ __device__ __forceinline__ void cl_sincosf(float x, float* sp, float* cp)
 {
     const double xd = (double)x;
     if (!(fabs(xd) <= 1.0e4)) {
-        *sp = __double2float_rn(sin(xd));
-        *cp = __double2float_rn(cos(xd));
+        const float2 sc = slow_sincosf(x);
+        *sp = sc.x;
+        *cp = sc.y;
         return;
     }
     if (xd == 0.0) {                           // sin(+-0) = +-0, cos(+-0) = 1
@@ -227,22 +255,34 @@ __device__ __forceinline__ bool fresnel(float n1, float n2, float cosi, float& R
 
 __device__ __forceinline__ int face_axis(int32_t face) { return face <= 2 ? 1 : (face <= 4 ? 2 : 3); }
 
+// specular, src/optics.jl:25-28.
 __device__ __forceinline__ void specular(float& ux, float& uy, float& uz, int32_t face)
 {
     const int a = face_axis(face);
     if (a == 1) ux = -ux; else if (a == 2) uy = -uy; else uz = -uz;
 }
 
-// lambertian_dir, src/optics.jl:118-138.
-__device__ __forceinline__ void lambertian(Stream& s, const Physics& P, int32_t face,
-                                           float& ux, float& uy, float& uz)
+// wall_hit, src/geometry.jl:19-32.
+__device__ __forceinline__ int32_t wall_hit(const Physics& P, float x, float y, float z,
+                                            float ux, float uy, float uz, float& d)
 {
-    const float ct = sqrtf(randu(s, P.key0, P.key1));
+    const float inf = __int_as_float(0x7f800000);
+    const float dx = ux > 0.0f ? (P.L0 - x) / ux : (ux < 0.0f ? (-x) / ux : inf);
+    const float dy = uy > 0.0f ? (P.L1 - y) / uy : (uy < 0.0f ? (-y) / uy : inf);
+    const float dz = uz > 0.0f ? (P.L2 - z) / uz : (uz < 0.0f ? (-z) / uz : inf);
+    if (dx <= dy && dx <= dz) { d = dx; return ux > 0.0f ? FACE_XP : FACE_XM; }
+    if (dy <= dz)             { d = dy; return uy > 0.0f ? FACE_YP : FACE_YM; }
+    d = dz;
+    return uz > 0.0f ? FACE_BACK : FACE_FRONT;
+}
+
+// Direction about the inward normal of a face from cos(theta) = ct and the
+// azimuth's (sin, cos): the tail of lambertian_dir, src/optics.jl:119-137.
+__device__ __forceinline__ void lambertian_from(int32_t face, float ct, float sphi, float cphi,
+                                                float& ux, float& uy, float& uz)
+{
     const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
-    const float phi = TWO_PI_F * randu(s, P.key0, P.key1);
-    float sp, cp;
-    cl_sincosf(phi, &sp, &cp);
-    const float a = st * cp, b = st * sp;
+    const float a = st * cphi, b = st * sphi;
     switch (face) {
     case FACE_XP:   ux = -ct; uy = a;   uz = b;   break;
     case FACE_XM:   ux = ct;  uy = a;   uz = b;   break;
@@ -253,75 +293,13 @@ __device__ __forceinline__ void lambertian(Stream& s, const Physics& P, int32_t 
     }
 }
 
-// gaussian, src/optics.jl:38-39.
-__device__ __forceinline__ float gaussian(Stream& s, const Physics& P, const double2* tab)
+// The tail of rayleigh_dir, src/optics.jl:93-111: rotate u by the polar
+// cosine mu about itself with the azimuth's (sin, cos).
+__device__ __forceinline__ void rayleigh_rotate(float mu, float sphi, float cphi,
+                                                float& ux, float& uy, float& uz)
 {
-    const float u1 = randu(s, P.key0, P.key1);
-    const float l = cl_logf(u1, tab);
-    const float u2 = randu(s, P.key0, P.key1);
-    return sqrtf(-2.0f * l) * cl_cosf(TWO_PI_F * u2);
-}
-
-// surface_interact (UNIFIED specular lobe), src/optics.jl:49-81.
-// Returns transmitted; on reflection the direction is updated.
-__device__ __forceinline__ bool surface_interact(Stream& s, const Physics& P, const double2* tab,
-                                                 float& ux, float& uy, float& uz, int32_t face)
-{
-    const int a = face_axis(face);
-    const float sgn = (face == FACE_XP || face == FACE_YP || face == FACE_BACK) ? 1.0f : -1.0f;
-    const float Nx = a == 1 ? sgn : 0.0f;
-    const float Ny = a == 2 ? sgn : 0.0f;
-    const float Nz = a == 3 ? sgn : 0.0f;
-    for (int tries = 0; tries < 20; ++tries) {
-        const float alpha = P.sigma_alpha * fabsf(gaussian(s, P, tab));
-        if (alpha >= 1.2f) continue;
-        float sa, ca;
-        cl_sincosf(alpha, &sa, &ca);
-        const float phi = TWO_PI_F * randu(s, P.key0, P.key1);
-        float sp, cp;
-        cl_sincosf(phi, &sp, &cp);
-        const float b = sa * cp, c = sa * sp;
-        const float Nfx = a == 1 ? ca * sgn : b;
-        const float Nfy = a == 2 ? ca * sgn : (a == 1 ? b : c);
-        const float Nfz = a == 3 ? ca * sgn : c;
-        const float cosi = ux * Nfx + uy * Nfy + uz * Nfz;
-        if (cosi <= 0.0f) continue;
-        float R;
-        const bool tir = fresnel(P.n_crystal, 1.0f, cosi, R);
-        if (tir || randu(s, P.key0, P.key1) < R) {
-            const float rx = ux - (2.0f * cosi) * Nfx;
-            const float ry = uy - (2.0f * cosi) * Nfy;
-            const float rz = uz - (2.0f * cosi) * Nfz;
-            if (rx * Nx + ry * Ny + rz * Nz < 0.0f) {
-                ux = rx; uy = ry; uz = rz;
-                return false;
-            }
-        } else {
-            return true;
-        }
-    }
-    specular(ux, uy, uz, face);
-    return false;
-}
-
-// rayleigh_dir, src/optics.jl:87-112.  The rejection loop accepts with
-// probability >= 1/2 per pass; it is bounded for safety and reports a budget
-// overrun through `overrun` (never reached with a proper uniform stream).
-__device__ __forceinline__ void rayleigh(Stream& s, const Physics& P,
-                                         float& ux, float& uy, float& uz, bool& overrun)
-{
-    float mu = 0.0f;
-    int it = 0;
-    for (;;) {
-        mu = 1.0f - 2.0f * randu(s, P.key0, P.key1);
-        if (2.0f * randu(s, P.key0, P.key1) <= 1.0f + mu * mu) break;
-        if (++it >= 4096) { overrun = true; break; }
-    }
     const float st = sqrtf(fmaxf(0.0f, 1.0f - mu * mu));
-    const float phi = TWO_PI_F * randu(s, P.key0, P.key1);
-    float sp, cp;
-    cl_sincosf(phi, &sp, &cp);
-    const float cb = st * cp, sb = st * sp;
+    const float cb = st * cphi, sb = st * sphi;
     float t1x, t1y, t1z, inv;
     if (fabsf(uz) < 0.9f) {
         inv = 1.0f / sqrtf(ux * ux + uy * uy);
@@ -338,135 +316,6 @@ __device__ __forceinline__ void rayleigh(Stream& s, const Physics& P,
     const float vz = mu * uz + cb * t1z + sb * t2z;
     inv = 1.0f / sqrtf(vx * vx + vy * vy + vz * vz);
     ux = vx * inv; uy = vy * inv; uz = vz * inv;
-}
-
-// A photon in flight.
-struct Photon {
-    float x, y, z, ux, uy, uz, t;
-    int32_t bounces, nscat;
-    Stream rng;
-};
-
-// Photon generation (src/kernel.jl:162-180): isotropic direction
-// (src/generation.jl:4-9), then t = pt + (-tau)*log(u) if tau > 0.
-__device__ __forceinline__ void photon_start(Photon& ph, const Physics& P, const double2* tab,
-                                             uint64_t pid, float x, float y, float z, float pt)
-{
-    stream_init(ph.rng, pid);
-    ph.x = x; ph.y = y; ph.z = z;
-    const float uz = 1.0f - 2.0f * randu(ph.rng, P.key0, P.key1);
-    const float r = sqrtf(fmaxf(0.0f, 1.0f - uz * uz));
-    const float phi = TWO_PI_F * randu(ph.rng, P.key0, P.key1);
-    float sp, cp;
-    cl_sincosf(phi, &sp, &cp);
-    ph.ux = r * cp; ph.uy = r * sp; ph.uz = uz;
-    float t = pt;
-    if (P.tau > 0.0f) t += (-P.tau) * cl_logf(randu(ph.rng, P.key0, P.key1), tab);
-    ph.t = t;
-    ph.bounces = 0;
-    ph.nscat = 0;
-}
-
-// One iteration of the bounce loop, src/transport.jl:126-233 /
-// src/kernel.jl:185-299.  Returns the terminal status or ST_FLYING.  On
-// detection `idx` receives the signed 1-based SiPM index.
-__device__ __forceinline__ int32_t photon_step(Photon& ph, const Physics& P, const double2* tab,
-                                               int32_t& idx, bool& overrun)
-{
-    float& x = ph.x; float& y = ph.y; float& z = ph.z;
-    float& ux = ph.ux; float& uy = ph.uy; float& uz = ph.uz;
-    Stream& s = ph.rng;
-
-    // wall_hit, src/geometry.jl:19-32
-    const float dx = ux > 0.0f ? (P.L0 - x) / ux : (ux < 0.0f ? (-x) / ux : __int_as_float(0x7f800000));
-    const float dy = uy > 0.0f ? (P.L1 - y) / uy : (uy < 0.0f ? (-y) / uy : __int_as_float(0x7f800000));
-    const float dz = uz > 0.0f ? (P.L2 - z) / uz : (uz < 0.0f ? (-z) / uz : __int_as_float(0x7f800000));
-    float d;
-    int32_t face;
-    if (dx <= dy && dx <= dz) { d = dx; face = ux > 0.0f ? FACE_XP : FACE_XM; }
-    else if (dy <= dz)        { d = dy; face = uy > 0.0f ? FACE_YP : FACE_YM; }
-    else                      { d = dz; face = uz > 0.0f ? FACE_BACK : FACE_FRONT; }
-
-    // bulk competition
-    const float inf = __int_as_float(0x7f800000);
-    float d_abs = inf, d_ray = inf;
-    if (P.abs_finite) d_abs = (-P.abs_len) * cl_logf(randu(s, P.key0, P.key1), tab);
-    if (P.ray_finite) d_ray = (-P.ray_len) * cl_logf(randu(s, P.key0, P.key1), tab);
-    if (d_abs < d && d_abs <= d_ray) return ST_ABS_BULK;
-    if (d_ray < d) {
-        x += d_ray * ux; y += d_ray * uy; z += d_ray * uz;
-        ph.t += d_ray * P.inv_v;
-        rayleigh(s, P, ux, uy, uz, overrun);
-        ph.nscat += 1;
-        ph.bounces += 1;
-        return ph.bounces >= P.max_bounces ? ST_CAP : ST_FLYING;
-    }
-
-    // advance to the wall: clamp, then snap the hit axis
-    const float nx_ = x + d * ux, ny_ = y + d * uy, nz_ = z + d * uz;
-    x = nx_ > P.L0 ? P.L0 : (nx_ < 0.0f ? 0.0f : nx_);
-    y = ny_ > P.L1 ? P.L1 : (ny_ < 0.0f ? 0.0f : ny_);
-    z = nz_ > P.L2 ? P.L2 : (nz_ < 0.0f ? 0.0f : nz_);
-    const int a = face_axis(face);
-    if (a == 1)      x = face == FACE_XP ? P.L0 : 0.0f;
-    else if (a == 2) y = face == FACE_YP ? P.L1 : 0.0f;
-    else             z = face == FACE_BACK ? P.L2 : 0.0f;
-    ph.t += d * P.inv_v;
-    const float cosi = a == 1 ? fabsf(ux) : (a == 2 ? fabsf(uy) : fabsf(uz));
-
-    if (face == FACE_BACK || (P.two_sided && face == FACE_FRONT)) {
-        // readout face, src/transport.jl:161-185
-        float R;
-        const bool tir = fresnel(P.n_crystal, P.n_coupling, cosi, R);
-        if (tir || randu(s, P.key0, P.key1) < R) {
-            specular(ux, uy, uz, face);
-        } else if (!P.disc || (x - P.cx) * (x - P.cx) + (y - P.cy) * (y - P.cy) <= P.r2) {
-            if (randu(s, P.key0, P.key1) <= P.pde) {
-                int32_t ii = 1 + (int32_t)(x / P.pitch);
-                int32_t jj = 1 + (int32_t)(y / P.pitch);
-                ii = ii < P.nx ? ii : P.nx;
-                jj = jj < P.ny ? jj : P.ny;
-                const int32_t lin = (jj - 1) * P.nx + ii;
-                idx = face == FACE_FRONT ? -lin : lin;
-                return ST_DETECTED;
-            }
-            return ST_ABS_SIPM;
-        } else if (randu(s, P.key0, P.key1) <= P.sur_R) {
-            if (P.sur_specular) specular(ux, uy, uz, face);
-            else lambertian(s, P, face, ux, uy, uz);
-        } else {
-            return ST_ABS_SUR;
-        }
-    } else if (!P.air_gap) {
-        // front-painted wrap, src/transport.jl:186-198
-        if (randu(s, P.key0, P.key1) <= P.wrap_R) {
-            if (P.wrap_specular) specular(ux, uy, uz, face);
-            else lambertian(s, P, face, ux, uy, uz);
-        } else {
-            return ST_ABS_WALL;
-        }
-    } else {
-        // back-painted wrap, src/transport.jl:199-226
-        bool transmitted = false;
-        if (P.sigma_alpha > 0.0f) {
-            transmitted = surface_interact(s, P, tab, ux, uy, uz, face);
-        } else {
-            float R;
-            const bool tir = fresnel(P.n_crystal, 1.0f, cosi, R);
-            if (tir || randu(s, P.key0, P.key1) < R) specular(ux, uy, uz, face);
-            else transmitted = true;
-        }
-        if (transmitted) {
-            if (randu(s, P.key0, P.key1) <= P.wrap_R) {
-                if (P.wrap_specular) specular(ux, uy, uz, face);
-                else lambertian(s, P, face, ux, uy, uz);
-            } else {
-                return ST_ABS_WALL;
-            }
-        }
-    }
-    ph.bounces += 1;
-    return ph.bounces >= P.max_bounces ? ST_CAP : ST_FLYING;
 }
 
 // Order-preserving map of a float onto uint32 (for atomicMin on times).

@@ -97,18 +97,36 @@ __device__ __forceinline__ int64_t find_source(const int64_t* __restrict__ off, 
     return lo;
 }
 
+// Per-lane transport states of the warp loop.  One loop iteration moves each
+// active lane one state forward; a whole wall interaction (move, UNIFIED try,
+// wrap) completes in one iteration, so an iteration is about one photon-step.
+enum : int32_t {
+    S_IDLE = 0,   // no photon
+    S_INIT = 1,   // emission: direction and time (src/kernel.jl:173-180)
+    S_MOVE = 2,   // bulk competition + wall interaction (src/transport.jl:127-233)
+    S_UNI = 3,    // another UNIFIED try at the same wall (src/optics.jl:54-78)
+    S_RAY = 4,    // Rayleigh rejection sampling + rotation (src/optics.jl:87-112)
+    S_LAMB = 5,   // Lambertian re-injection (src/optics.jl:118-138)
+};
+// Uniforms one iteration can consume at most (move: abs, ray, 3 for the
+// UNIFIED try, Fresnel, wrap).  The ring is topped up to this before the
+// iteration's draws.
+constexpr int DRAWS_PER_ITER = 7;
+
 template <int MODE, bool REC, bool TILE>
 __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ KArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     double2* s_tab = reinterpret_cast<double2*>(smem);
-    uint32_t* s_counts = reinterpret_cast<uint32_t*>(smem + LOGTAB_BYTES);
+    uint32_t* s_ring = reinterpret_cast<uint32_t*>(smem + LOGTAB_BYTES);
+    uint32_t* s_counts = s_ring + RING_LEN * blockDim.x;
     uint32_t* s_keys = s_counts + (TILE ? A.cells * A.bins_total : 0);
     __shared__ unsigned long long s_cnt[10];
     __shared__ unsigned int s_last;
 
     const Physics& P = A.P;
     const int tid = threadIdx.x;
+    const int stride = blockDim.x;
     for (int i = tid; i < CLM_LOG_NTAB; i += blockDim.x)
         s_tab[i] = make_double2(c_logtab[2 * i], c_logtab[2 * i + 1]);
     if (TILE) {
@@ -121,23 +139,29 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
 
     uint32_t* tile_counts = TILE ? s_counts : A.counts;
     uint32_t* tile_keys = TILE ? s_keys : A.keys;
+    uint32_t* ring = s_ring + tid;
 
     const int lane = tid & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
+    const bool uni_possible = P.air_gap && P.sigma_alpha > 0.0f;
+    const float inf = __int_as_float(0x7f800000);
 
-    Photon ph;
-    bool active = false;
+    // per-lane photon state
+    float x = 0.f, y = 0.f, z = 0.f, ux = 0.f, uy = 0.f, uz = 0.f, t = 0.f;
+    float carry = 0.f;                 // uz (init), mu (Rayleigh), u1 (Lambertian)
+    int32_t bounces = 0, nscat = 0, st = S_IDLE, face = 0, tries = 0;
+    Rng rng;
+    rng_init(rng, 0);
     int64_t k = 0;
     int32_t seg = 0;
-    int64_t pool_lo = 0, pool_hi = 0, pool_src = 0;   // warp-uniform
-    bool exhausted = false;                           // warp-uniform
-    uint32_t n_det = 0, n_front = 0, n_bulk = 0, n_wall = 0, n_sipm = 0, n_cap = 0, n_sur = 0;
-    unsigned long long c_scat = 0, c_sumb = 0, c_steps = 0;
-    bool overrun = false;
+    // warp-uniform work pool
+    int64_t pool_lo = 0, pool_hi = 0, pool_src = 0;
+    bool exhausted = false;
+    bool overrun = false, under = false;
 
     for (;;) {
         // ---- refill idle lanes from the warp's pool / the global queue ----
-        const unsigned need = __ballot_sync(FULL, !active);
+        const unsigned need = __ballot_sync(FULL, st == S_IDLE);
         if (need != 0u && !exhausted) {
             const int nneed = __popc(need);
             const int rank = __popc(need & lt_mask);
@@ -145,7 +169,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
             int64_t my_hint = pool_src;
             const int64_t avail = pool_hi - pool_lo;
             const int64_t taken = avail < nneed ? avail : (int64_t)nneed;
-            if (!active && rank < taken) my_k = pool_lo + rank;
+            if (st == S_IDLE && rank < taken) my_k = pool_lo + rank;
             pool_lo += taken;
             if (taken < nneed) {
                 unsigned long long base = 0;
@@ -165,7 +189,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
                     const int64_t rem = nneed - taken;
                     const int64_t avail2 = pool_hi - pool_lo;
                     const int64_t taken2 = avail2 < rem ? avail2 : rem;
-                    if (!active && rank >= taken && rank - taken < taken2) {
+                    if (st == S_IDLE && rank >= taken && rank - taken < taken2) {
                         my_k = pool_lo + (rank - taken);
                         my_hint = pool_src;
                     }
@@ -174,29 +198,241 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
             }
             if (my_k >= 0) {
                 k = my_k;
-                float sx, sy, sz, st;
                 if (MODE == 0) {
                     const int32_t j = A.npos == 1 ? 0 : (int32_t)((uint64_t)k % (uint64_t)A.npos);
-                    sx = __ldg(A.px + j); sy = __ldg(A.py + j); sz = __ldg(A.pz + j);
-                    st = A.pt ? __ldg(A.pt + j) : 0.0f;
+                    x = __ldg(A.px + j); y = __ldg(A.py + j); z = __ldg(A.pz + j);
+                    t = A.pt ? __ldg(A.pt + j) : 0.0f;
                 } else {
                     const int64_t s = find_source(A.src_off, A.n_src, my_hint, k);
-                    sx = __ldg(A.px + s); sy = __ldg(A.py + s); sz = __ldg(A.pz + s);
-                    st = A.pt ? __ldg(A.pt + s) : 0.0f;
+                    x = __ldg(A.px + s); y = __ldg(A.py + s); z = __ldg(A.pz + s);
+                    t = A.pt ? __ldg(A.pt + s) : 0.0f;
                     seg = __ldg(A.src_seg + s);
                 }
-                photon_start(ph, P, s_tab, A.pid0 + (uint64_t)k + 1ull, sx, sy, sz, st);
-                active = true;
+                rng_init(rng, A.pid0 + (uint64_t)k + 1ull);
+                bounces = 0; nscat = 0; tries = 0;
+                st = S_INIT;
             }
         }
-        if (!__any_sync(FULL, active)) break;
+        if (!__any_sync(FULL, st != S_IDLE)) break;
 
-        // ---- one bounce-loop iteration per active lane ----
+        // ---- top up the uniform ring: one Philox call site for the warp ----
+#pragma unroll 1
+        for (int r = 0; r < 2; ++r) {
+            const bool want = st != S_IDLE && rng.cnt < DRAWS_PER_ITER;
+            if (__any_sync(FULL, want)) {
+                if (want) rng_fill(rng, ring, stride, P.key0, P.key1);
+            }
+        }
+
+        // ---- pre: draw uniforms, stage arguments of the elementary functions ----
+        float a0 = 1.f, a1 = 1.f, a2 = 1.f, p0 = 1.f, p1 = 1.f;
+        bool nl0 = false, nl1 = false, nl2 = false, ns0 = false, ns1 = false;
+        bool ray_ok = false;
+        if (st == S_INIT) {
+            carry = 1.0f - 2.0f * rng_pop(rng, ring, stride, under);       // uz
+            p1 = TWO_PI_F * rng_pop(rng, ring, stride, under); ns1 = true;  // azimuth
+            if (P.tau > 0.0f) { a0 = rng_pop(rng, ring, stride, under); nl0 = true; }
+        } else if (st == S_MOVE || st == S_UNI) {
+            if (st == S_MOVE) {
+                if (P.abs_finite) { a0 = rng_pop(rng, ring, stride, under); nl0 = true; }
+                if (P.ray_finite) { a1 = rng_pop(rng, ring, stride, under); nl1 = true; }
+            }
+            if (uni_possible) {
+                // speculative: the next three uniforms are the UNIFIED try's
+                // gaussian pair and facet azimuth if this step reaches a wrap
+                a2 = rng_peek(rng, ring, stride, 0u); nl2 = true;
+                p0 = TWO_PI_F * rng_peek(rng, ring, stride, 1u); ns0 = true;
+                p1 = TWO_PI_F * rng_peek(rng, ring, stride, 2u); ns1 = true;
+            }
+        } else if (st == S_RAY) {
+            const float mu = 1.0f - 2.0f * rng_pop(rng, ring, stride, under);
+            ray_ok = 2.0f * rng_pop(rng, ring, stride, under) <= 1.0f + mu * mu;
+            carry = mu;
+            if (ray_ok) { p1 = TWO_PI_F * rng_pop(rng, ring, stride, under); ns1 = true; }
+        } else if (st == S_LAMB) {
+            carry = rng_pop(rng, ring, stride, under);                       // u for cos(theta)
+            p1 = TWO_PI_F * rng_pop(rng, ring, stride, under); ns1 = true;
+        }
+
+        // ---- elementary functions, once per warp (Float64, rounded once) ----
+        float L0 = 0.f, L1 = 0.f, L2 = 0.f, s0 = 0.f, c0 = 1.f, s1 = 0.f, c1 = 1.f;
+        if (__any_sync(FULL, nl0)) L0 = cl_logf(a0, s_tab);
+        if (__any_sync(FULL, nl1)) L1 = cl_logf(a1, s_tab);
+        if (__any_sync(FULL, nl2)) L2 = cl_logf(a2, s_tab);
+        if (__any_sync(FULL, ns0)) cl_sincosf(p0, &s0, &c0);
+        if (__any_sync(FULL, ns1)) cl_sincosf(p1, &s1, &c1);
+
+        // ---- post, part 1 ----
         int32_t status = ST_FLYING, idx = 0;
-        if (active) {
-            stream_topup(ph.rng, P.key0, P.key1);
-            status = photon_step(ph, P, s_tab, idx, overrun);
-            c_steps += 1ull;
+        bool uni = false, wall_done = false, to_wrap = false;
+        if (st == S_INIT) {
+            const float r = sqrtf(fmaxf(0.0f, 1.0f - carry * carry));
+            ux = r * c1; uy = r * s1; uz = carry;
+            if (P.tau > 0.0f) t += (-P.tau) * L0;
+            st = S_MOVE;
+        } else if (st == S_MOVE) {
+            float d;
+            const int32_t f = wall_hit(P, x, y, z, ux, uy, uz, d);
+            const float d_abs = P.abs_finite ? (-P.abs_len) * L0 : inf;
+            const float d_ray = P.ray_finite ? (-P.ray_len) * L1 : inf;
+            if (d_abs < d && d_abs <= d_ray) {
+                status = ST_ABS_BULK;
+            } else if (d_ray < d) {
+                x += d_ray * ux; y += d_ray * uy; z += d_ray * uz;
+                t += d_ray * P.inv_v;
+                st = S_RAY;
+                tries = 0;
+            } else {
+                // advance to the wall: clamp, then snap the hit axis (src/transport.jl:146-157)
+                const float nx_ = x + d * ux, ny_ = y + d * uy, nz_ = z + d * uz;
+                x = nx_ > P.L0 ? P.L0 : (nx_ < 0.0f ? 0.0f : nx_);
+                y = ny_ > P.L1 ? P.L1 : (ny_ < 0.0f ? 0.0f : ny_);
+                z = nz_ > P.L2 ? P.L2 : (nz_ < 0.0f ? 0.0f : nz_);
+                const int a = face_axis(f);
+                if (a == 1)      x = f == FACE_XP ? P.L0 : 0.0f;
+                else if (a == 2) y = f == FACE_YP ? P.L1 : 0.0f;
+                else             z = f == FACE_BACK ? P.L2 : 0.0f;
+                t += d * P.inv_v;
+                const float cosi = a == 1 ? fabsf(ux) : (a == 2 ? fabsf(uy) : fabsf(uz));
+                face = f;
+                if (f == FACE_BACK || (P.two_sided && f == FACE_FRONT)) {
+                    // readout face, src/transport.jl:161-185
+                    float R;
+                    const bool tir = fresnel(P.n_crystal, P.n_coupling, cosi, R);
+                    if (tir || rng_pop(rng, ring, stride, under) < R) {
+                        specular(ux, uy, uz, f);
+                        wall_done = true;
+                    } else if (!P.disc || (x - P.cx) * (x - P.cx) + (y - P.cy) * (y - P.cy) <= P.r2) {
+                        if (rng_pop(rng, ring, stride, under) <= P.pde) {
+                            int32_t ii = 1 + (int32_t)(x / P.pitch);
+                            int32_t jj = 1 + (int32_t)(y / P.pitch);
+                            ii = ii < P.nx ? ii : P.nx;
+                            jj = jj < P.ny ? jj : P.ny;
+                            const int32_t lin = (jj - 1) * P.nx + ii;
+                            idx = f == FACE_FRONT ? -lin : lin;
+                            status = ST_DETECTED;
+                        } else {
+                            status = ST_ABS_SIPM;
+                        }
+                    } else if (rng_pop(rng, ring, stride, under) <= P.sur_R) {
+                        if (P.sur_specular) { specular(ux, uy, uz, f); wall_done = true; }
+                        else st = S_LAMB;
+                    } else {
+                        status = ST_ABS_SUR;
+                    }
+                } else if (!P.air_gap) {
+                    // front-painted wrap, src/transport.jl:186-198
+                    if (rng_pop(rng, ring, stride, under) <= P.wrap_R) {
+                        if (P.wrap_specular) { specular(ux, uy, uz, f); wall_done = true; }
+                        else st = S_LAMB;
+                    } else {
+                        status = ST_ABS_WALL;
+                    }
+                } else if (P.sigma_alpha > 0.0f) {
+                    tries = 0;
+                    uni = true;                      // UNIFIED lobe, below
+                } else {
+                    float R;
+                    const bool tir = fresnel(P.n_crystal, 1.0f, cosi, R);
+                    if (tir || rng_pop(rng, ring, stride, under) < R) {
+                        specular(ux, uy, uz, f);
+                        wall_done = true;
+                    } else {
+                        to_wrap = true;
+                    }
+                }
+            }
+        } else if (st == S_UNI) {
+            uni = true;
+        } else if (st == S_RAY) {
+            if (ray_ok || ++tries >= 4096) {
+                overrun |= !ray_ok;
+                rayleigh_rotate(carry, s1, c1, ux, uy, uz);
+                nscat += 1;
+                bounces += 1;
+                if (bounces >= P.max_bounces) status = ST_CAP;
+                else st = S_MOVE;
+            }
+        } else if (st == S_LAMB) {
+            lambertian_from(face, sqrtf(carry), s1, c1, ux, uy, uz);
+            wall_done = true;
+        }
+
+        // UNIFIED try, first half (src/optics.jl:55-56): the gaussian tilt
+        bool facet = false;
+        float alpha = 0.f;
+        if (uni) {
+            rng_pop(rng, ring, stride, under);       // gaussian u1 (its log is L2)
+            rng_pop(rng, ring, stride, under);       // gaussian u2 (its cos is c0)
+            alpha = P.sigma_alpha * fabsf(sqrtf(-2.0f * L2) * c0);
+            if (alpha >= 1.2f) {
+                if (++tries >= 20) { specular(ux, uy, uz, face); wall_done = true; st = S_MOVE; }
+                else st = S_UNI;
+            } else {
+                rng_pop(rng, ring, stride, under);   // facet azimuth (its sincos is s1, c1)
+                facet = true;
+            }
+        }
+
+        // ---- facet tilt sin/cos, once per warp ----
+        float sa = 0.f, ca = 1.f;
+        if (__any_sync(FULL, facet)) cl_sincosf(facet ? alpha : 1.0f, &sa, &ca);
+
+        // UNIFIED try, second half (src/optics.jl:57-77): facet, Fresnel, reflection
+        if (facet) {
+            const int a = face_axis(face);
+            const float sgn = (face == FACE_XP || face == FACE_YP || face == FACE_BACK) ? 1.0f : -1.0f;
+            const float Nx = a == 1 ? sgn : 0.0f;
+            const float Ny = a == 2 ? sgn : 0.0f;
+            const float Nz = a == 3 ? sgn : 0.0f;
+            const float b = sa * c1, c = sa * s1;
+            const float Nfx = a == 1 ? ca * sgn : b;
+            const float Nfy = a == 2 ? ca * sgn : (a == 1 ? b : c);
+            const float Nfz = a == 3 ? ca * sgn : c;
+            const float cosi = ux * Nfx + uy * Nfy + uz * Nfz;
+            bool retry = false;
+            if (cosi <= 0.0f) {
+                retry = true;
+            } else {
+                float R;
+                const bool tir = fresnel(P.n_crystal, 1.0f, cosi, R);
+                if (tir || rng_pop(rng, ring, stride, under) < R) {
+                    const float rx = ux - (2.0f * cosi) * Nfx;
+                    const float ry = uy - (2.0f * cosi) * Nfy;
+                    const float rz = uz - (2.0f * cosi) * Nfz;
+                    if (rx * Nx + ry * Ny + rz * Nz < 0.0f) {
+                        ux = rx; uy = ry; uz = rz;
+                        wall_done = true;
+                        st = S_MOVE;
+                    } else {
+                        retry = true;
+                    }
+                } else {
+                    to_wrap = true;
+                    st = S_MOVE;
+                }
+            }
+            if (retry) {
+                if (++tries >= 20) { specular(ux, uy, uz, face); wall_done = true; st = S_MOVE; }
+                else st = S_UNI;
+            }
+        }
+
+        // transmitted into the air gap: the reflector (src/transport.jl:214-225)
+        if (to_wrap) {
+            if (rng_pop(rng, ring, stride, under) <= P.wrap_R) {
+                if (P.wrap_specular) { specular(ux, uy, uz, face); wall_done = true; }
+                else st = S_LAMB;
+            } else {
+                status = ST_ABS_WALL;
+            }
+        }
+
+        // end of a wall interaction: count the bounce (src/transport.jl:228-232)
+        if (wall_done && status == ST_FLYING) {
+            bounces += 1;
+            if (bounces >= P.max_bounces) status = ST_CAP;
+            else st = S_MOVE;
         }
 
         // ---- detections: warp-aggregated atomics ----
@@ -205,9 +441,9 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
         if (det) {
             const int32_t lin = idx < 0 ? -idx : idx;
             const int32_t cell = lin - 1;
-            const uint32_t key = float_key(ph.t);
+            const uint32_t key = float_key(t);
             if (MODE == 0) {
-                const int32_t slot = cell + A.cells * time_bin0(ph.t, P);
+                const int32_t slot = cell + A.cells * time_bin0(t, P);
                 const unsigned g = __match_any_sync(dmask, slot);
                 if (lane == __ffs(g) - 1) atomicAdd(tile_counts + slot, (uint32_t)__popc(g));
                 atomicMin(tile_keys + cell, key);
@@ -220,56 +456,37 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
             }
         }
 
-        // ---- terminal bookkeeping ----
-        if (status != ST_FLYING) {
-            switch (status) {
-            case ST_DETECTED:
-                n_det += 1u; c_sumb += (unsigned long long)ph.bounces;
-                if (idx < 0) n_front += 1u;
-                break;
-            case ST_ABS_BULK: n_bulk += 1u; break;
-            case ST_ABS_WALL: n_wall += 1u; break;
-            case ST_ABS_SIPM: n_sipm += 1u; break;
-            case ST_ABS_SUR:  n_sur += 1u; break;
-            default:          n_cap += 1u; break;
+        // ---- terminal bookkeeping: warp-aggregated counters ----
+        const bool term = status != ST_FLYING;
+        const unsigned tmask = __ballot_sync(FULL, term);
+        if (tmask != 0u) {
+            if (term) {
+                const unsigned g = __match_any_sync(tmask, status);
+                // counters[] order: ndet, ndet_front, bulk, wall, sipm, cap, sur
+                const int slot = status == ST_DETECTED ? 0 : (status == ST_ABS_SUR ? 6 : status);
+                if (lane == __ffs(g) - 1) atomicAdd(&s_cnt[slot], (unsigned long long)__popc(g));
+                if (REC) {
+                    if (A.r_status) A.r_status[k] = (uint8_t)status;
+                    if (A.r_idx) A.r_idx[k] = (int16_t)idx;
+                    if (A.r_t) A.r_t[k] = t;
+                    if (A.r_bounces) A.r_bounces[k] = bounces;
+                }
             }
-            c_scat += (unsigned long long)ph.nscat;
-            if (REC) {
-                if (A.r_status) A.r_status[k] = (uint8_t)status;
-                if (A.r_idx) A.r_idx[k] = (int16_t)idx;
-                if (A.r_t) A.r_t[k] = ph.t;
-                if (A.r_bounces) A.r_bounces[k] = ph.bounces;
+            const unsigned front = __ballot_sync(FULL, det && idx < 0);
+            const uint32_t sb = __reduce_add_sync(FULL, det ? (uint32_t)bounces : 0u);
+            const uint32_t sc = __reduce_add_sync(FULL, term ? (uint32_t)nscat : 0u);
+            const uint32_t ss = __reduce_add_sync(FULL, term ? (uint32_t)(bounces + (status != ST_CAP)) : 0u);
+            if (lane == 0) {
+                if (front) atomicAdd(&s_cnt[1], (unsigned long long)__popc(front));
+                if (sc) atomicAdd(&s_cnt[7], (unsigned long long)sc);
+                if (sb) atomicAdd(&s_cnt[8], (unsigned long long)sb);
+                atomicAdd(&s_cnt[9], (unsigned long long)ss);
             }
-            active = false;
+            if (term) st = S_IDLE;
         }
     }
-
-    // ---- CTA reduction of the counters ----
-    {
-        const uint32_t v0 = __reduce_add_sync(FULL, n_det);
-        const uint32_t v1 = __reduce_add_sync(FULL, n_front);
-        const uint32_t v2 = __reduce_add_sync(FULL, n_bulk);
-        const uint32_t v3 = __reduce_add_sync(FULL, n_wall);
-        const uint32_t v4 = __reduce_add_sync(FULL, n_sipm);
-        const uint32_t v5 = __reduce_add_sync(FULL, n_cap);
-        const uint32_t v6 = __reduce_add_sync(FULL, n_sur);
-        const unsigned long long v7 = warp_sum_u64(c_scat);
-        const unsigned long long v8 = warp_sum_u64(c_sumb);
-        const unsigned long long v9 = warp_sum_u64(c_steps);
-        if (lane == 0) {
-            if (v0) atomicAdd(&s_cnt[0], (unsigned long long)v0);
-            if (v1) atomicAdd(&s_cnt[1], (unsigned long long)v1);
-            if (v2) atomicAdd(&s_cnt[2], (unsigned long long)v2);
-            if (v3) atomicAdd(&s_cnt[3], (unsigned long long)v3);
-            if (v4) atomicAdd(&s_cnt[4], (unsigned long long)v4);
-            if (v5) atomicAdd(&s_cnt[5], (unsigned long long)v5);
-            if (v6) atomicAdd(&s_cnt[6], (unsigned long long)v6);
-            if (v7) atomicAdd(&s_cnt[7], v7);
-            if (v8) atomicAdd(&s_cnt[8], v8);
-            if (v9) atomicAdd(&s_cnt[9], v9);
-        }
-        if (overrun) atomicOr(A.err, 1u);
-    }
+    if (overrun) atomicOr(A.err, 1u);
+    if (under) atomicOr(A.err, 2u);
     __syncthreads();
 
     // ---- one coalesced flush per CTA ----
@@ -377,12 +594,11 @@ __global__ void debug_randu_kernel(float* out, int64_t n, int32_t n_per, uint32_
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        Stream s;
-        stream_init(s, (uint64_t)i + 1ull);
-        for (int32_t j = 0; j < n_per; ++j) {
-            if ((j % 3) == 0) stream_topup(s, k0, k1);   // exercise both buffer paths
-            out[i * n_per + j] = randu(s, k0, k1);
-        }
+        SimpleStream s;
+        const uint64_t pid = (uint64_t)i + 1ull;
+        s.pid_lo = (uint32_t)pid; s.pid_hi = (uint32_t)(pid >> 32); s.block = 0; s.n = 0;
+        s.b0 = s.b1 = s.b2 = s.b3 = 0;
+        for (int32_t j = 0; j < n_per; ++j) out[i * n_per + j] = simple_randu(s, k0, k1);
     }
 }
 
@@ -657,8 +873,9 @@ static int enqueue_point(cl_handle* h, const Physics& P, const float* px, const 
     if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
     a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
     const size_t tile_bytes = ((size_t)n_counts + cells) * sizeof(uint32_t);
-    const bool tile = LOGTAB_BYTES + tile_bytes <= (size_t)std::min(h->max_smem_optin, 160 * 1024);
-    const size_t smem = LOGTAB_BYTES + (tile ? tile_bytes : 0);
+    const size_t base_bytes = LOGTAB_BYTES + (size_t)RING_LEN * h->threads * sizeof(uint32_t);
+    const bool tile = base_bytes + tile_bytes <= (size_t)std::min(h->max_smem_optin, 160 * 1024);
+    const size_t smem = base_bytes + (tile ? tile_bytes : 0);
     if (tile) return want_rec ? launch_transport<0, true, true>(h, a, smem, st)
                               : launch_transport<0, false, true>(h, a, smem, st);
     return want_rec ? launch_transport<0, true, false>(h, a, smem, st)
@@ -688,8 +905,9 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
         const bool want_rec = rec && (rec->status || rec->idx || rec->t || rec->bounces);
         if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
         a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
-        const int rc = want_rec ? launch_transport<1, true, false>(h, a, LOGTAB_BYTES, st)
-                                : launch_transport<1, false, false>(h, a, LOGTAB_BYTES, st);
+        const size_t smem = LOGTAB_BYTES + (size_t)RING_LEN * h->threads * sizeof(uint32_t);
+        const int rc = want_rec ? launch_transport<1, true, false>(h, a, smem, st)
+                                : launch_transport<1, false, false>(h, a, smem, st);
         if (rc != CL_OK) return rc;
     }
     finalize_segments<<<(unsigned)std::min<int64_t>((total + 255) / 256 + 1, 8192), 256, 0, st>>>(
@@ -707,6 +925,7 @@ static int collect(cl_handle* h, cudaStream_t st)
     CK(h, cudaMemcpyAsync(&err, s.err, sizeof err, cudaMemcpyDeviceToHost, st), "copy status");
     CK(h, cudaStreamSynchronize(st), "stream synchronize");
     h->last_steps = (int64_t)steps;
+    if (err & 2u) return set_err(h, CL_ERR_CUDA, "internal error: uniform ring underflow in the transport kernel");
     if (err) return set_err(h, CL_ERR_TIMEOUT, "a device-side loop budget ran out (Rayleigh rejection sampler)");
     return CL_OK;
 }
