@@ -42,6 +42,22 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
     return c;
 }
 
+// The same rounds with the key schedule (k0 + r*W0, k1 + r*W1, r = 0..9)
+// precomputed: rk[2r], rk[2r+1].  With rk in the constant bank the XORs take
+// their key operand straight from it.
+__device__ __forceinline__ uint4 philox4x32_10_rk(uint4 c, const uint32_t* __restrict__ rk)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)PHILOX_M0 * c.x;
+        const uint64_t p1 = (uint64_t)PHILOX_M1 * c.z;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c = make_uint4(hi1 ^ c.y ^ rk[2 * r], lo1, hi0 ^ c.w ^ rk[2 * r + 1], lo0);
+    }
+    return c;
+}
+
 // randu, src/philox.jl:62: ((x >>> 8) + 1.0f0) * 2^-24, exact, in (0, 1].
 __device__ __forceinline__ float u32_to_randu(uint32_t x)
 {
@@ -72,9 +88,9 @@ __device__ __forceinline__ void rng_init(Rng& r, uint64_t pid)
     r.cnt = 0;
 }
 
-__device__ __forceinline__ void rng_fill(Rng& r, uint32_t* ring, int stride, uint32_t k0, uint32_t k1)
+__device__ __forceinline__ void rng_fill(Rng& r, uint32_t* ring, int stride, const uint32_t* rk)
 {
-    const uint4 o = philox4x32_10(make_uint4(r.pid_lo, r.pid_hi, r.block, 0u), k0, k1);
+    const uint4 o = philox4x32_10_rk(make_uint4(r.pid_lo, r.pid_hi, r.block, 0u), rk);
     r.block += 1u;
     const uint32_t w = r.head + (uint32_t)r.cnt;
     ring[((w + 0u) % RING_LEN) * stride] = o.x;
@@ -167,9 +183,61 @@ __device__ __forceinline__ float cl_logf(float x, const double2* __restrict__ ta
     return __double2float_rn(res);
 }
 
-// sin and cos together.  Cody-Waite reduction x = q pi/2 + r with a two-term
-// pi/2, |r| <= pi/4, then Taylor polynomials (sin to r^17, cos to r^16).
-__device__ __forceinline__ void cl_sincosf(float x, float* sp, float* cp)
+// log of a uniform ((x>>8)+1)*2^-24: always a positive normal float, so the
+// domain check of cl_logf is not needed.
+__device__ __forceinline__ float cl_logf_u(float x, const double2* __restrict__ tab)
+{
+    const uint32_t b = __float_as_uint(x);
+    int e = (int)(b >> 23) - 127;
+    uint32_t mb = b & 0x007fffffu;
+    const int hi = mb >= 0x3504f3u;
+    e += hi;
+    mb |= hi ? 0x3f000000u : 0x3f800000u;
+    const double m = (double)__uint_as_float(mb);
+    const int j = __double2int_rn((m - 1.0) * 64.0);
+    const double F = 1.0 + (double)j * 0.015625;
+    const double2 t = tab[j - CLM_LOG_JMIN];
+    const double r = (m - F) * t.x;
+    double p = CLM_L8;
+    p = fma(p, r, CLM_L7);
+    p = fma(p, r, CLM_L6);
+    p = fma(p, r, CLM_L5);
+    p = fma(p, r, CLM_L4);
+    p = fma(p, r, CLM_L3);
+    p = fma(p, r, CLM_L2);
+    const double lp = fma(p * r, r, r);
+    const double res = fma((double)e, CLM_LN2, t.y) + lp;
+    return __double2float_rn(res);
+}
+
+// sin and cos together, table-driven: x = j*delta + r with delta = 2 pi/256
+// (two-term delta, |r| <= pi/256), (sin, cos)(j*delta) from a 256-entry table
+// in shared memory, sin r and cos r - 1 by their Taylor series to r^7 and r^8,
+// recombined as S + (S (cos r - 1) + C sin r) and C + (C (cos r - 1) - S sin r).
+// The table-driven core for 0 <= x <= 1e4 (the transport passes azimuths
+// 2*pi*u in (0, 2*pi] and facet tilts in [0, 1.2)); +0 maps to (+0, 1).
+__device__ __forceinline__ void cl_sincosf_core(float x, const double2* __restrict__ sctab,
+                                                float* sp, float* cp)
+{
+    const double xd = (double)x;
+    const double n = rint(xd * CLM_SC_INV_DELTA);
+    double r = fma(-n, CLM_SC_DELTA_HI, xd);
+    r = fma(-n, CLM_SC_DELTA_LO, r);
+    const double2 sc = sctab[(int)n & (CLM_SC_N - 1)];
+    const double r2 = r * r;
+    double ps = fma(CLM_TS7, r2, CLM_TS5);
+    ps = fma(ps, r2, CLM_TS3);
+    const double sr = fma(r * r2, ps, r);
+    double pc = fma(CLM_TC8, r2, CLM_TC6);
+    pc = fma(pc, r2, CLM_TC4);
+    pc = fma(pc, r2, CLM_TC2);
+    const double cm1 = r2 * pc;
+    *sp = __double2float_rn(sc.x + fma(sc.x, cm1, sc.y * sr));
+    *cp = __double2float_rn(sc.y + fma(sc.y, cm1, -(sc.x * sr)));
+}
+
+__device__ __forceinline__ void cl_sincosf(float x, const double2* __restrict__ sctab,
+                                           float* sp, float* cp)
 {
     const double xd = (double)x;
     if (!(fabs(xd) <= 1.0e4)) {
@@ -183,39 +251,25 @@ __device__ __forceinline__ void cl_sincosf(float x, float* sp, float* cp)
         *cp = 1.0f;
         return;
     }
-    const double q = rint(xd * CLM_2_OVER_PI);
-    double r = fma(-q, CLM_PIO2_HI, xd);
-    r = fma(-q, CLM_PIO2_LO, r);
+    const double n = rint(xd * CLM_SC_INV_DELTA);
+    double r = fma(-n, CLM_SC_DELTA_HI, xd);
+    r = fma(-n, CLM_SC_DELTA_LO, r);
+    const double2 sc = sctab[(int)n & (CLM_SC_N - 1)];
     const double r2 = r * r;
-    double ps = CLM_S17;
-    ps = fma(ps, r2, CLM_S15);
-    ps = fma(ps, r2, CLM_S13);
-    ps = fma(ps, r2, CLM_S11);
-    ps = fma(ps, r2, CLM_S9);
-    ps = fma(ps, r2, CLM_S7);
-    ps = fma(ps, r2, CLM_S5);
-    ps = fma(ps, r2, CLM_S3);
-    const double sn = fma(r * r2, ps, r);
-    double pc = CLM_C16;
-    pc = fma(pc, r2, CLM_C14);
-    pc = fma(pc, r2, CLM_C12);
-    pc = fma(pc, r2, CLM_C10);
-    pc = fma(pc, r2, CLM_C8);
-    pc = fma(pc, r2, CLM_C6);
-    pc = fma(pc, r2, CLM_C4);
-    pc = fma(pc, r2, CLM_C2);
-    const double cs = fma(r2, pc, 1.0);
-    const int iq = (int)q;
-    double s = (iq & 1) ? cs : sn;
-    double c = (iq & 1) ? sn : cs;
-    if (iq & 2) s = -s;
-    if ((iq + 1) & 2) c = -c;
+    double ps = fma(CLM_TS7, r2, CLM_TS5);
+    ps = fma(ps, r2, CLM_TS3);
+    const double sr = fma(r * r2, ps, r);      // sin r
+    double pc = fma(CLM_TC8, r2, CLM_TC6);
+    pc = fma(pc, r2, CLM_TC4);
+    pc = fma(pc, r2, CLM_TC2);
+    const double cm1 = r2 * pc;                // cos r - 1
+    const double s = sc.x + fma(sc.x, cm1, sc.y * sr);
+    const double c = sc.y + fma(sc.y, cm1, -(sc.x * sr));
     *sp = __double2float_rn(s);
     *cp = __double2float_rn(c);
 }
 
-__device__ __forceinline__ float cl_sinf(float x) { float s, c; cl_sincosf(x, &s, &c); return s; }
-__device__ __forceinline__ float cl_cosf(float x) { float s, c; cl_sincosf(x, &s, &c); return c; }
+
 
 // ---------------------------------------------------------------------------
 // Transport parameters (flattened OpticalParams / Readout / TimeBinning / Box).
@@ -227,6 +281,8 @@ struct Physics {
     float cx, cy, r2, sur_R, pitch, bin_ns, tau;
     int32_t nx, ny, nbins, max_bounces;
     uint32_t key0, key1;
+    uint32_t rk[20];             // Philox round keys
+    float qc2, qa2;              // (n_crystal/n_coupling)^2, (n_crystal/1)^2
     uint8_t abs_finite, ray_finite, wrap_specular, air_gap;
     uint8_t disc, sur_specular, two_sided, pad_;
 };
@@ -245,6 +301,19 @@ __device__ __forceinline__ bool fresnel(float n1, float n2, float cosi, float& R
 {
     const float q = n1 / n2;
     const float sin2t = (q * q) * (1.0f - cosi * cosi);
+    if (sin2t >= 1.0f) { R = 1.0f; return true; }
+    const float cost = sqrtf(1.0f - sin2t);
+    const float a = (n1 * cosi - n2 * cost) / (n1 * cosi + n2 * cost);
+    const float b = (n1 * cost - n2 * cosi) / (n1 * cost + n2 * cosi);
+    R = 0.5f * (a * a + b * b);
+    return false;
+}
+
+// fresnel with (n1/n2)^2 precomputed (the same Float32 value the reference
+// computes each call).
+__device__ __forceinline__ bool fresnel_q2(float n1, float n2, float q2, float cosi, float& R)
+{
+    const float sin2t = q2 * (1.0f - cosi * cosi);
     if (sin2t >= 1.0f) { R = 1.0f; return true; }
     const float cost = sqrtf(1.0f - sin2t);
     const float a = (n1 * cosi - n2 * cost) / (n1 * cosi + n2 * cost);

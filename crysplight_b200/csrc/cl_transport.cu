@@ -36,9 +36,22 @@
 namespace cl {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int LOGTAB_BYTES = ((CLM_LOG_NTAB * 16 + 127) / 128) * 128;
+constexpr int SCTAB_BYTES = CLM_SC_N * 16;
+constexpr int LOGTAB_BYTES = ((CLM_LOG_NTAB * 16 + 127) / 128) * 128 + SCTAB_BYTES;  // both tables
 
 __constant__ double c_logtab[2 * CLM_LOG_NTAB] = { CLM_LOG_TAB_INIT };
+__constant__ double c_sctab[2 * CLM_SC_N] = { CLM_SC_TAB_INIT };
+
+// Copy the log and sincos tables into shared memory (the first LOGTAB_BYTES).
+__device__ __forceinline__ void load_tables(unsigned char* smem, double2*& tab, double2*& sctab)
+{
+    sctab = reinterpret_cast<double2*>(smem);
+    tab = reinterpret_cast<double2*>(smem + SCTAB_BYTES);
+    for (int i = threadIdx.x; i < CLM_SC_N; i += blockDim.x)
+        sctab[i] = make_double2(c_sctab[2 * i], c_sctab[2 * i + 1]);
+    for (int i = threadIdx.x; i < CLM_LOG_NTAB; i += blockDim.x)
+        tab[i] = make_double2(c_logtab[2 * i], c_logtab[2 * i + 1]);
+}
 
 struct KArgs {
     Physics P;
@@ -112,12 +125,15 @@ enum : int32_t {
 // UNIFIED try, Fresnel, wrap).  The ring is topped up to this before the
 // iteration's draws.
 constexpr int DRAWS_PER_ITER = 7;
+// Fresnel interfaces met in an iteration (one evaluation serves all three).
+enum : int32_t { FK_NONE = 0, FK_READOUT = 1, FK_POLISHED = 2, FK_FACET = 3 };
 
 template <int MODE, bool REC, bool TILE>
 __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ KArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    double2* s_tab = reinterpret_cast<double2*>(smem);
+    double2 *s_tab, *s_sctab;
+    load_tables(smem, s_tab, s_sctab);
     uint32_t* s_ring = reinterpret_cast<uint32_t*>(smem + LOGTAB_BYTES);
     uint32_t* s_counts = s_ring + RING_LEN * blockDim.x;
     uint32_t* s_keys = s_counts + (TILE ? A.cells * A.bins_total : 0);
@@ -127,8 +143,6 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
     const Physics& P = A.P;
     const int tid = threadIdx.x;
     const int stride = blockDim.x;
-    for (int i = tid; i < CLM_LOG_NTAB; i += blockDim.x)
-        s_tab[i] = make_double2(c_logtab[2 * i], c_logtab[2 * i + 1]);
     if (TILE) {
         const int nt = A.cells * A.bins_total;
         for (int i = tid; i < nt; i += blockDim.x) s_counts[i] = 0u;
@@ -220,7 +234,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
         for (int r = 0; r < 2; ++r) {
             const bool want = st != S_IDLE && rng.cnt < DRAWS_PER_ITER;
             if (__any_sync(FULL, want)) {
-                if (want) rng_fill(rng, ring, stride, P.key0, P.key1);
+                if (want) rng_fill(rng, ring, stride, P.rk);
             }
         }
 
@@ -256,15 +270,17 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
 
         // ---- elementary functions, once per warp (Float64, rounded once) ----
         float L0 = 0.f, L1 = 0.f, L2 = 0.f, s0 = 0.f, c0 = 1.f, s1 = 0.f, c1 = 1.f;
-        if (__any_sync(FULL, nl0)) L0 = cl_logf(a0, s_tab);
-        if (__any_sync(FULL, nl1)) L1 = cl_logf(a1, s_tab);
-        if (__any_sync(FULL, nl2)) L2 = cl_logf(a2, s_tab);
-        if (__any_sync(FULL, ns0)) cl_sincosf(p0, &s0, &c0);
-        if (__any_sync(FULL, ns1)) cl_sincosf(p1, &s1, &c1);
+        if (__any_sync(FULL, nl0)) L0 = cl_logf_u(a0, s_tab);
+        if (__any_sync(FULL, nl1)) L1 = cl_logf_u(a1, s_tab);
+        if (__any_sync(FULL, nl2)) L2 = cl_logf_u(a2, s_tab);
+        if (__any_sync(FULL, ns0)) cl_sincosf_core(p0, s_sctab, &s0, &c0);
+        if (__any_sync(FULL, ns1)) cl_sincosf_core(p1, s_sctab, &s1, &c1);
 
         // ---- post, part 1 ----
         int32_t status = ST_FLYING, idx = 0;
         bool uni = false, wall_done = false, to_wrap = false;
+        int32_t fk = FK_NONE;                  // which Fresnel interface this lane meets
+        float fn2 = 1.0f, fq2 = 1.0f, fcos = 1.0f;
         if (st == S_INIT) {
             const float r = sqrtf(fmaxf(0.0f, 1.0f - carry * carry));
             ux = r * c1; uy = r * s1; uz = carry;
@@ -296,30 +312,8 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
                 const float cosi = a == 1 ? fabsf(ux) : (a == 2 ? fabsf(uy) : fabsf(uz));
                 face = f;
                 if (f == FACE_BACK || (P.two_sided && f == FACE_FRONT)) {
-                    // readout face, src/transport.jl:161-185
-                    float R;
-                    const bool tir = fresnel(P.n_crystal, P.n_coupling, cosi, R);
-                    if (tir || rng_pop(rng, ring, stride, under) < R) {
-                        specular(ux, uy, uz, f);
-                        wall_done = true;
-                    } else if (!P.disc || (x - P.cx) * (x - P.cx) + (y - P.cy) * (y - P.cy) <= P.r2) {
-                        if (rng_pop(rng, ring, stride, under) <= P.pde) {
-                            int32_t ii = 1 + (int32_t)(x / P.pitch);
-                            int32_t jj = 1 + (int32_t)(y / P.pitch);
-                            ii = ii < P.nx ? ii : P.nx;
-                            jj = jj < P.ny ? jj : P.ny;
-                            const int32_t lin = (jj - 1) * P.nx + ii;
-                            idx = f == FACE_FRONT ? -lin : lin;
-                            status = ST_DETECTED;
-                        } else {
-                            status = ST_ABS_SIPM;
-                        }
-                    } else if (rng_pop(rng, ring, stride, under) <= P.sur_R) {
-                        if (P.sur_specular) { specular(ux, uy, uz, f); wall_done = true; }
-                        else st = S_LAMB;
-                    } else {
-                        status = ST_ABS_SUR;
-                    }
+                    // readout face, src/transport.jl:161-185: Fresnel below
+                    fk = FK_READOUT; fn2 = P.n_coupling; fq2 = P.qc2; fcos = cosi;
                 } else if (!P.air_gap) {
                     // front-painted wrap, src/transport.jl:186-198
                     if (rng_pop(rng, ring, stride, under) <= P.wrap_R) {
@@ -332,14 +326,8 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
                     tries = 0;
                     uni = true;                      // UNIFIED lobe, below
                 } else {
-                    float R;
-                    const bool tir = fresnel(P.n_crystal, 1.0f, cosi, R);
-                    if (tir || rng_pop(rng, ring, stride, under) < R) {
-                        specular(ux, uy, uz, f);
-                        wall_done = true;
-                    } else {
-                        to_wrap = true;
-                    }
+                    // polished back-painted face, src/transport.jl:206-212: Fresnel below
+                    fk = FK_POLISHED; fn2 = 1.0f; fq2 = P.qa2; fcos = cosi;
                 }
             }
         } else if (st == S_UNI) {
@@ -376,30 +364,68 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
 
         // ---- facet tilt sin/cos, once per warp ----
         float sa = 0.f, ca = 1.f;
-        if (__any_sync(FULL, facet)) cl_sincosf(facet ? alpha : 1.0f, &sa, &ca);
+        if (__any_sync(FULL, facet)) cl_sincosf_core(facet ? alpha : 1.0f, s_sctab, &sa, &ca);
 
-        // UNIFIED try, second half (src/optics.jl:57-77): facet, Fresnel, reflection
+        // UNIFIED try, second half (src/optics.jl:57-66): the facet normal
+        float Nfx = 0.f, Nfy = 0.f, Nfz = 0.f;
+        bool retry = false;
         if (facet) {
             const int a = face_axis(face);
             const float sgn = (face == FACE_XP || face == FACE_YP || face == FACE_BACK) ? 1.0f : -1.0f;
-            const float Nx = a == 1 ? sgn : 0.0f;
-            const float Ny = a == 2 ? sgn : 0.0f;
-            const float Nz = a == 3 ? sgn : 0.0f;
             const float b = sa * c1, c = sa * s1;
-            const float Nfx = a == 1 ? ca * sgn : b;
-            const float Nfy = a == 2 ? ca * sgn : (a == 1 ? b : c);
-            const float Nfz = a == 3 ? ca * sgn : c;
+            Nfx = a == 1 ? ca * sgn : b;
+            Nfy = a == 2 ? ca * sgn : (a == 1 ? b : c);
+            Nfz = a == 3 ? ca * sgn : c;
             const float cosi = ux * Nfx + uy * Nfy + uz * Nfz;
-            bool retry = false;
-            if (cosi <= 0.0f) {
-                retry = true;
+            if (cosi <= 0.0f) retry = true;
+            else { fk = FK_FACET; fn2 = 1.0f; fq2 = P.qa2; fcos = cosi; }
+        }
+
+        // ---- Fresnel (src/optics.jl:10-19), one evaluation per warp ----
+        float R = 1.0f;
+        bool tir = true;
+        if (__any_sync(FULL, fk != FK_NONE)) {
+            if (fk != FK_NONE) tir = fresnel_q2(P.n_crystal, fn2, fq2, fcos, R);
+        }
+        if (fk != FK_NONE) {
+            const bool refl = tir || rng_pop(rng, ring, stride, under) < R;
+            if (fk == FK_READOUT) {
+                if (refl) {
+                    specular(ux, uy, uz, face);
+                    wall_done = true;
+                } else if (!P.disc || (x - P.cx) * (x - P.cx) + (y - P.cy) * (y - P.cy) <= P.r2) {
+                    if (rng_pop(rng, ring, stride, under) <= P.pde) {
+                        int32_t ii = 1 + (int32_t)(x / P.pitch);
+                        int32_t jj = 1 + (int32_t)(y / P.pitch);
+                        ii = ii < P.nx ? ii : P.nx;
+                        jj = jj < P.ny ? jj : P.ny;
+                        const int32_t lin = (jj - 1) * P.nx + ii;
+                        idx = face == FACE_FRONT ? -lin : lin;
+                        status = ST_DETECTED;
+                    } else {
+                        status = ST_ABS_SIPM;
+                    }
+                } else if (rng_pop(rng, ring, stride, under) <= P.sur_R) {
+                    if (P.sur_specular) { specular(ux, uy, uz, face); wall_done = true; }
+                    else st = S_LAMB;
+                } else {
+                    status = ST_ABS_SUR;
+                }
+            } else if (fk == FK_POLISHED) {
+                if (refl) { specular(ux, uy, uz, face); wall_done = true; }
+                else to_wrap = true;
             } else {
-                float R;
-                const bool tir = fresnel(P.n_crystal, 1.0f, cosi, R);
-                if (tir || rng_pop(rng, ring, stride, under) < R) {
-                    const float rx = ux - (2.0f * cosi) * Nfx;
-                    const float ry = uy - (2.0f * cosi) * Nfy;
-                    const float rz = uz - (2.0f * cosi) * Nfz;
+                // facet: reflect about the facet normal; keep it only if it
+                // points back into the crystal (src/optics.jl:68-77)
+                if (refl) {
+                    const int a = face_axis(face);
+                    const float sgn = (face == FACE_XP || face == FACE_YP || face == FACE_BACK) ? 1.0f : -1.0f;
+                    const float Nx = a == 1 ? sgn : 0.0f;
+                    const float Ny = a == 2 ? sgn : 0.0f;
+                    const float Nz = a == 3 ? sgn : 0.0f;
+                    const float rx = ux - (2.0f * fcos) * Nfx;
+                    const float ry = uy - (2.0f * fcos) * Nfy;
+                    const float rz = uz - (2.0f * fcos) * Nfz;
                     if (rx * Nx + ry * Ny + rz * Nz < 0.0f) {
                         ux = rx; uy = ry; uz = rz;
                         wall_done = true;
@@ -412,10 +438,10 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
                     st = S_MOVE;
                 }
             }
-            if (retry) {
-                if (++tries >= 20) { specular(ux, uy, uz, face); wall_done = true; st = S_MOVE; }
-                else st = S_UNI;
-            }
+        }
+        if (retry) {
+            if (++tries >= 20) { specular(ux, uy, uz, face); wall_done = true; st = S_MOVE; }
+            else st = S_UNI;
         }
 
         // transmitted into the air gap: the reflector (src/transport.jl:214-225)
@@ -562,17 +588,21 @@ __global__ void decode_keys_kernel(uint32_t* keys, int64_t n)
 // ---- diagnostics ----
 __global__ void debug_math_kernel(int fn, const float* in, float* out, int64_t n)
 {
-    __shared__ double2 s_tab[CLM_LOG_NTAB];
-    for (int i = threadIdx.x; i < CLM_LOG_NTAB; i += blockDim.x)
-        s_tab[i] = make_double2(c_logtab[2 * i], c_logtab[2 * i + 1]);
+    __shared__ __align__(16) unsigned char tabs[LOGTAB_BYTES];
+    double2 *s_tab, *s_sctab;
+    load_tables(tabs, s_tab, s_sctab);
     __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const float x = in[i];
         float r;
-        if (fn == 0) r = cl_logf(x, s_tab);
-        else if (fn == 1) r = cl_sinf(x);
-        else r = cl_cosf(x);
+        if (fn == 0) {
+            r = cl_logf(x, s_tab);
+        } else {
+            float sv, cv;
+            cl_sincosf(x, s_sctab, &sv, &cv);
+            r = fn == 1 ? sv : cv;
+        }
         out[i] = r;
     }
 }
@@ -798,6 +828,17 @@ static Physics make_physics(const cl_box* box, const cl_optical_params* op, cons
     P.pitch = ro->grid.pitch_mm; P.bin_ns = tb->bin_ns; P.tau = tau_ns;
     P.nx = ro->grid.nx; P.ny = ro->grid.ny; P.nbins = tb->nbins; P.max_bounces = max_bounces;
     P.key0 = (uint32_t)seed; P.key1 = (uint32_t)(seed >> 32);
+    {
+        uint32_t k0 = P.key0, k1 = P.key1;
+        for (int r = 0; r < 10; ++r) {
+            P.rk[2 * r] = k0; P.rk[2 * r + 1] = k1;
+            k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+        }
+        const float qc = op->n_crystal / op->n_coupling;   // IEEE division on the host, as on the device
+        const float qa = op->n_crystal / 1.0f;
+        P.qc2 = qc * qc;
+        P.qa2 = qa * qa;
+    }
     P.abs_finite = std::isfinite(op->abs_len_mm) ? 1 : 0;
     P.ray_finite = std::isfinite(op->rayleigh_mm) ? 1 : 0;
     P.wrap_specular = op->wrap_specular ? 1 : 0;

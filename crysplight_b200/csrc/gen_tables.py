@@ -38,6 +38,23 @@ def d_pi() -> Decimal:
     return 16 * atan_inv(5) - 4 * atan_inv(239)
 
 
+def d_sin_cos(x: Decimal) -> tuple:
+    """sin and cos by their Taylor series at 60 digits (|x| <= 2 pi)."""
+    eps = Decimal(10) ** (-(getcontext().prec + 2))
+    s, c = Decimal(0), Decimal(0)
+    term, n = Decimal(1), 0          # x^n / n!
+    while True:
+        if n % 4 == 0: c += term
+        elif n % 4 == 1: s += term
+        elif n % 4 == 2: c -= term
+        else: s -= term
+        n += 1
+        term = term * x / n
+        if abs(term) < eps and n > 4:
+            break
+    return s, c
+
+
 def dbl(x: Decimal) -> float:
     return float(x)
 
@@ -85,6 +102,33 @@ def main() -> None:
         inv = dbl(1 / F)
         lg = dbl(F.ln()) if j != 0 else 0.0
         out.append(f"    {hexd(inv)}, {hexd(lg)},  /* j = {j} */ \\")
+    out.append("")
+    # table-driven sincos: x = j*delta + r, delta = 2 pi / 256, |r| <= delta/2
+    n_sc = 256
+    delta = 2 * pi / n_sc
+    d_hi = dbl(delta)
+    d_lo = dbl(delta - Decimal(d_hi))
+    out.append("")
+    out.append(f"#define CLM_SC_N {n_sc}")
+    out.append(f"#define CLM_SC_DELTA_HI {hexd(d_hi)}")
+    out.append(f"#define CLM_SC_DELTA_LO {hexd(d_lo)}")
+    out.append(f"#define CLM_SC_INV_DELTA {hexd(dbl(1 / delta))}")
+    for n in (3, 5, 7):
+        c = Decimal((-1) ** ((n - 1) // 2)) / Decimal(math.factorial(n))
+        out.append(f"#define CLM_TS{n} {hexd(dbl(c))}")
+    for n in (2, 4, 6, 8):
+        c = Decimal((-1) ** (n // 2)) / Decimal(math.factorial(n))
+        out.append(f"#define CLM_TC{n} {hexd(dbl(c))}")
+    out.append("/* (sin, cos)(j * 2 pi / 256), j = 0..255; exact zeros where the value is 0 */")
+    out.append("#define CLM_SC_TAB_INIT \\")
+    for j in range(n_sc):
+        if j % 64 == 0:
+            sj, cj = (0.0, [1.0, 0.0, -1.0, 0.0][j // 64]) if j % 128 == 0 else (
+                [0.0, 1.0, 0.0, -1.0][j // 64], 0.0)
+        else:
+            sd, cd = d_sin_cos(delta * j)
+            sj, cj = dbl(sd), dbl(cd)
+        out.append(f"    {hexd(sj)}, {hexd(cj)},  /* j = {j} */ \\")
     out.append("")
     print("\n".join(out))
 
