@@ -13,7 +13,7 @@ import threading
 from .params import Box, Counters, OpticalParams, Readout, Records, TimeBinning
 
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
-LIB_PATH = os.path.join(LIB_DIR, "libcrysplight_cuda.so")
+LIB_PATH = os.environ.get("CRYSPLIGHT_CUDA_LIB") or os.path.join(LIB_DIR, "libcrysplight_cuda.so")
 
 # Exported symbols, exactly those declared in include/crysplight_cuda.h.
 EXPORTS = (

@@ -65,13 +65,14 @@ __device__ __forceinline__ float u32_to_randu(uint32_t x)
 }
 
 // A photon's uniform stream (PhiloxStream, src/philox.jl:34-62): key = seed,
-// counter = (pid lo, pid hi, block, 0).  The outputs are buffered in a
-// per-lane ring of RING_LEN words in shared memory (word i of lane `tid` at
-// ring[(i % RING_LEN) * blockDim + tid]: every access is bank-conflict free).
-// Blocks are generated ahead of use, at one convergent point of the warp
-// loop; pop() consumes in order and peek(d) looks d words ahead, so the
-// sequence of uniforms is exactly the reference's.
+// counter = (pid lo, pid hi, block, 0).  The uniforms are buffered, already
+// converted by randu, in a per-lane ring of RING_LEN floats in shared memory:
+// word i of the lane at column `tid` sits at ring[(i % RING_LEN) * RING_STRIDE]
+// (every access is bank-conflict free).  Blocks are generated ahead of use, at
+// one convergent point of the warp loop; pop() consumes in order and peek(d)
+// looks d words ahead, so the sequence of uniforms is exactly the reference's.
 constexpr int RING_LEN = 16;
+constexpr int RING_STRIDE = 256;      // columns: the largest block the kernels launch
 
 struct Rng {
     uint32_t pid_lo, pid_hi, block;
@@ -88,29 +89,35 @@ __device__ __forceinline__ void rng_init(Rng& r, uint64_t pid)
     r.cnt = 0;
 }
 
-__device__ __forceinline__ void rng_fill(Rng& r, uint32_t* ring, int stride, const uint32_t* rk)
+// Two consecutive blocks at once (independent Philox chains interleave).
+// Requires cnt <= RING_LEN - 8.
+__device__ __forceinline__ void rng_fill2(Rng& r, float* ring, const uint32_t* rk)
 {
     const uint4 o = philox4x32_10_rk(make_uint4(r.pid_lo, r.pid_hi, r.block, 0u), rk);
-    r.block += 1u;
+    const uint4 q = philox4x32_10_rk(make_uint4(r.pid_lo, r.pid_hi, r.block + 1u, 0u), rk);
+    r.block += 2u;
     const uint32_t w = r.head + (uint32_t)r.cnt;
-    ring[((w + 0u) % RING_LEN) * stride] = o.x;
-    ring[((w + 1u) % RING_LEN) * stride] = o.y;
-    ring[((w + 2u) % RING_LEN) * stride] = o.z;
-    ring[((w + 3u) % RING_LEN) * stride] = o.w;
-    r.cnt += 4;
+    ring[((w + 0u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o.x);
+    ring[((w + 1u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o.y);
+    ring[((w + 2u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o.z);
+    ring[((w + 3u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o.w);
+    ring[((w + 4u) % RING_LEN) * RING_STRIDE] = u32_to_randu(q.x);
+    ring[((w + 5u) % RING_LEN) * RING_STRIDE] = u32_to_randu(q.y);
+    ring[((w + 6u) % RING_LEN) * RING_STRIDE] = u32_to_randu(q.z);
+    ring[((w + 7u) % RING_LEN) * RING_STRIDE] = u32_to_randu(q.w);
+    r.cnt += 8;
 }
 
-__device__ __forceinline__ float rng_peek(const Rng& r, const uint32_t* ring, int stride, uint32_t d)
+__device__ __forceinline__ float rng_peek(const Rng& r, const float* ring, uint32_t d)
 {
-    return u32_to_randu(ring[((r.head + d) % RING_LEN) * stride]);
+    return ring[((r.head + d) % RING_LEN) * RING_STRIDE];
 }
 
 // Pop the next uniform.  The warp loop keeps at least as many words buffered
-// as one iteration can consume; `under` records a violation of that bound.
-__device__ __forceinline__ float rng_pop(Rng& r, const uint32_t* ring, int stride, bool& under)
+// as one iteration can consume (checked once per iteration through cnt).
+__device__ __forceinline__ float rng_pop(Rng& r, const float* ring)
 {
-    under |= r.cnt <= 0;
-    const float u = u32_to_randu(ring[(r.head % RING_LEN) * stride]);
+    const float u = ring[(r.head % RING_LEN) * RING_STRIDE];
     r.head += 1u;
     r.cnt -= 1;
     return u;

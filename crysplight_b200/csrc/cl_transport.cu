@@ -128,14 +128,18 @@ constexpr int DRAWS_PER_ITER = 7;
 // Fresnel interfaces met in an iteration (one evaluation serves all three).
 enum : int32_t { FK_NONE = 0, FK_READOUT = 1, FK_POLISHED = 2, FK_FACET = 3 };
 
+#ifndef CL_MIN_CTAS_PER_SM
+#define CL_MIN_CTAS_PER_SM 4
+#endif
+
 template <int MODE, bool REC, bool TILE>
-__global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ KArgs A)
+__global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(const __grid_constant__ KArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     double2 *s_tab, *s_sctab;
     load_tables(smem, s_tab, s_sctab);
-    uint32_t* s_ring = reinterpret_cast<uint32_t*>(smem + LOGTAB_BYTES);
-    uint32_t* s_counts = s_ring + RING_LEN * blockDim.x;
+    float* s_ring = reinterpret_cast<float*>(smem + LOGTAB_BYTES);
+    uint32_t* s_counts = reinterpret_cast<uint32_t*>(s_ring + RING_LEN * RING_STRIDE);
     uint32_t* s_keys = s_counts + (TILE ? A.cells * A.bins_total : 0);
     __shared__ unsigned long long s_cnt[10];
     __shared__ unsigned int s_last;
@@ -153,7 +157,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
 
     uint32_t* tile_counts = TILE ? s_counts : A.counts;
     uint32_t* tile_keys = TILE ? s_keys : A.keys;
-    uint32_t* ring = s_ring + tid;
+    float* ring = s_ring + tid;
 
     const int lane = tid & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -230,11 +234,10 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
         if (!__any_sync(FULL, st != S_IDLE)) break;
 
         // ---- top up the uniform ring: one Philox call site for the warp ----
-#pragma unroll 1
-        for (int r = 0; r < 2; ++r) {
+        {
             const bool want = st != S_IDLE && rng.cnt < DRAWS_PER_ITER;
             if (__any_sync(FULL, want)) {
-                if (want) rng_fill(rng, ring, stride, P.rk);
+                if (want) rng_fill2(rng, ring, P.rk);
             }
         }
 
@@ -243,38 +246,42 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
         bool nl0 = false, nl1 = false, nl2 = false, ns0 = false, ns1 = false;
         bool ray_ok = false;
         if (st == S_INIT) {
-            carry = 1.0f - 2.0f * rng_pop(rng, ring, stride, under);       // uz
-            p1 = TWO_PI_F * rng_pop(rng, ring, stride, under); ns1 = true;  // azimuth
-            if (P.tau > 0.0f) { a0 = rng_pop(rng, ring, stride, under); nl0 = true; }
+            carry = 1.0f - 2.0f * rng_pop(rng, ring);       // uz
+            p1 = TWO_PI_F * rng_pop(rng, ring); ns1 = true;  // azimuth
+            if (P.tau > 0.0f) { a0 = rng_pop(rng, ring); nl0 = true; }
         } else if (st == S_MOVE || st == S_UNI) {
             if (st == S_MOVE) {
-                if (P.abs_finite) { a0 = rng_pop(rng, ring, stride, under); nl0 = true; }
-                if (P.ray_finite) { a1 = rng_pop(rng, ring, stride, under); nl1 = true; }
+                if (P.abs_finite) { a0 = rng_pop(rng, ring); nl0 = true; }
+                if (P.ray_finite) { a1 = rng_pop(rng, ring); nl1 = true; }
             }
             if (uni_possible) {
                 // speculative: the next three uniforms are the UNIFIED try's
                 // gaussian pair and facet azimuth if this step reaches a wrap
-                a2 = rng_peek(rng, ring, stride, 0u); nl2 = true;
-                p0 = TWO_PI_F * rng_peek(rng, ring, stride, 1u); ns0 = true;
-                p1 = TWO_PI_F * rng_peek(rng, ring, stride, 2u); ns1 = true;
+                a2 = rng_peek(rng, ring, 0u); nl2 = true;
+                p0 = TWO_PI_F * rng_peek(rng, ring, 1u); ns0 = true;
+                p1 = TWO_PI_F * rng_peek(rng, ring, 2u); ns1 = true;
             }
         } else if (st == S_RAY) {
-            const float mu = 1.0f - 2.0f * rng_pop(rng, ring, stride, under);
-            ray_ok = 2.0f * rng_pop(rng, ring, stride, under) <= 1.0f + mu * mu;
+            const float mu = 1.0f - 2.0f * rng_pop(rng, ring);
+            ray_ok = 2.0f * rng_pop(rng, ring) <= 1.0f + mu * mu;
             carry = mu;
-            if (ray_ok) { p1 = TWO_PI_F * rng_pop(rng, ring, stride, under); ns1 = true; }
+            if (ray_ok) { p1 = TWO_PI_F * rng_pop(rng, ring); ns1 = true; }
         } else if (st == S_LAMB) {
-            carry = rng_pop(rng, ring, stride, under);                       // u for cos(theta)
-            p1 = TWO_PI_F * rng_pop(rng, ring, stride, under); ns1 = true;
+            carry = rng_pop(rng, ring);                       // u for cos(theta)
+            p1 = TWO_PI_F * rng_pop(rng, ring); ns1 = true;
         }
 
         // ---- elementary functions, once per warp (Float64, rounded once) ----
-        float L0 = 0.f, L1 = 0.f, L2 = 0.f, s0 = 0.f, c0 = 1.f, s1 = 0.f, c1 = 1.f;
-        if (__any_sync(FULL, nl0)) L0 = cl_logf_u(a0, s_tab);
-        if (__any_sync(FULL, nl1)) L1 = cl_logf_u(a1, s_tab);
-        if (__any_sync(FULL, nl2)) L2 = cl_logf_u(a2, s_tab);
-        if (__any_sync(FULL, ns0)) cl_sincosf_core(p0, s_sctab, &s0, &c0);
-        if (__any_sync(FULL, ns1)) cl_sincosf_core(p1, s_sctab, &s1, &c1);
+        // Straight-line and unconditional: the five evaluations are independent,
+        // so their Float64 dependency chains interleave (lanes that need none of
+        // them get the harmless argument 1).
+        float L0, L1, L2, s0, c0, s1, c1;
+        L0 = cl_logf_u(a0, s_tab);
+        L1 = cl_logf_u(a1, s_tab);
+        L2 = cl_logf_u(a2, s_tab);
+        cl_sincosf_core(p0, s_sctab, &s0, &c0);
+        cl_sincosf_core(p1, s_sctab, &s1, &c1);
+        (void)nl0; (void)nl1; (void)nl2; (void)ns0; (void)ns1;
 
         // ---- post, part 1 ----
         int32_t status = ST_FLYING, idx = 0;
@@ -316,7 +323,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
                     fk = FK_READOUT; fn2 = P.n_coupling; fq2 = P.qc2; fcos = cosi;
                 } else if (!P.air_gap) {
                     // front-painted wrap, src/transport.jl:186-198
-                    if (rng_pop(rng, ring, stride, under) <= P.wrap_R) {
+                    if (rng_pop(rng, ring) <= P.wrap_R) {
                         if (P.wrap_specular) { specular(ux, uy, uz, f); wall_done = true; }
                         else st = S_LAMB;
                     } else {
@@ -350,21 +357,23 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
         bool facet = false;
         float alpha = 0.f;
         if (uni) {
-            rng_pop(rng, ring, stride, under);       // gaussian u1 (its log is L2)
-            rng_pop(rng, ring, stride, under);       // gaussian u2 (its cos is c0)
+            rng_pop(rng, ring);       // gaussian u1 (its log is L2)
+            rng_pop(rng, ring);       // gaussian u2 (its cos is c0)
             alpha = P.sigma_alpha * fabsf(sqrtf(-2.0f * L2) * c0);
             if (alpha >= 1.2f) {
                 if (++tries >= 20) { specular(ux, uy, uz, face); wall_done = true; st = S_MOVE; }
                 else st = S_UNI;
             } else {
-                rng_pop(rng, ring, stride, under);   // facet azimuth (its sincos is s1, c1)
+                rng_pop(rng, ring);   // facet azimuth (its sincos is s1, c1)
                 facet = true;
             }
         }
 
         // ---- facet tilt sin/cos, once per warp ----
         float sa = 0.f, ca = 1.f;
-        if (__any_sync(FULL, facet)) cl_sincosf_core(facet ? alpha : 1.0f, s_sctab, &sa, &ca);
+        if (__any_sync(FULL, facet)) {
+            cl_sincosf_core(facet ? alpha : 1.0f, s_sctab, &sa, &ca);
+        }
 
         // UNIFIED try, second half (src/optics.jl:57-66): the facet normal
         float Nfx = 0.f, Nfy = 0.f, Nfz = 0.f;
@@ -388,13 +397,13 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
             if (fk != FK_NONE) tir = fresnel_q2(P.n_crystal, fn2, fq2, fcos, R);
         }
         if (fk != FK_NONE) {
-            const bool refl = tir || rng_pop(rng, ring, stride, under) < R;
+            const bool refl = tir || rng_pop(rng, ring) < R;
             if (fk == FK_READOUT) {
                 if (refl) {
                     specular(ux, uy, uz, face);
                     wall_done = true;
                 } else if (!P.disc || (x - P.cx) * (x - P.cx) + (y - P.cy) * (y - P.cy) <= P.r2) {
-                    if (rng_pop(rng, ring, stride, under) <= P.pde) {
+                    if (rng_pop(rng, ring) <= P.pde) {
                         int32_t ii = 1 + (int32_t)(x / P.pitch);
                         int32_t jj = 1 + (int32_t)(y / P.pitch);
                         ii = ii < P.nx ? ii : P.nx;
@@ -405,7 +414,7 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
                     } else {
                         status = ST_ABS_SIPM;
                     }
-                } else if (rng_pop(rng, ring, stride, under) <= P.sur_R) {
+                } else if (rng_pop(rng, ring) <= P.sur_R) {
                     if (P.sur_specular) { specular(ux, uy, uz, face); wall_done = true; }
                     else st = S_LAMB;
                 } else {
@@ -446,13 +455,15 @@ __global__ void __launch_bounds__(256) transport_kernel(const __grid_constant__ 
 
         // transmitted into the air gap: the reflector (src/transport.jl:214-225)
         if (to_wrap) {
-            if (rng_pop(rng, ring, stride, under) <= P.wrap_R) {
+            if (rng_pop(rng, ring) <= P.wrap_R) {
                 if (P.wrap_specular) { specular(ux, uy, uz, face); wall_done = true; }
                 else st = S_LAMB;
             } else {
                 status = ST_ABS_WALL;
             }
         }
+
+        under |= rng.cnt < 0;
 
         // end of a wall interaction: count the bounce (src/transport.jl:228-232)
         if (wall_done && status == ST_FLYING) {
@@ -914,7 +925,7 @@ static int enqueue_point(cl_handle* h, const Physics& P, const float* px, const 
     if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
     a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
     const size_t tile_bytes = ((size_t)n_counts + cells) * sizeof(uint32_t);
-    const size_t base_bytes = LOGTAB_BYTES + (size_t)RING_LEN * h->threads * sizeof(uint32_t);
+    const size_t base_bytes = LOGTAB_BYTES + (size_t)RING_LEN * RING_STRIDE * sizeof(float);
     const bool tile = base_bytes + tile_bytes <= (size_t)std::min(h->max_smem_optin, 160 * 1024);
     const size_t smem = base_bytes + (tile ? tile_bytes : 0);
     if (tile) return want_rec ? launch_transport<0, true, true>(h, a, smem, st)
@@ -946,7 +957,7 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
         const bool want_rec = rec && (rec->status || rec->idx || rec->t || rec->bounces);
         if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
         a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
-        const size_t smem = LOGTAB_BYTES + (size_t)RING_LEN * h->threads * sizeof(uint32_t);
+        const size_t smem = LOGTAB_BYTES + (size_t)RING_LEN * RING_STRIDE * sizeof(float);
         const int rc = want_rec ? launch_transport<1, true, false>(h, a, smem, st)
                                 : launch_transport<1, false, false>(h, a, smem, st);
         if (rc != CL_OK) return rc;

@@ -256,7 +256,8 @@ int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta,
  * Diagnostics for tests: evaluate the device's Float32 elementary functions
  * on n inputs.  fn: 0 = log, 1 = sin, 2 = cos, 3 = Philox4x32-10 on
  * (in_u32[4k..4k+3] counter, key = (seed lo, hi)) -> out_u32[4k..4k+3],
- * 4 = randu stream: out[k*m + i] = i-th uniform of pid = k + 1 (m = n_per).
+ * 4 = randu stream: out[k*m + i] = i-th uniform of pid = k + 1 (m = n_per),
+ * 5 = cuRAND's Philox4x32-10 on the same inputs as 3 (cross-check).
  * Host buffers, synchronous.
  */
 int cl_debug_eval(cl_handle* h, int fn, const void* in, void* out, int64_t n,

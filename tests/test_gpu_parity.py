@@ -140,6 +140,10 @@ CASES = {
                                                    (3.0, 40.0, 1.0)],
                                         t0s=[0.0, 55.5, 7000.0], pid_offset=123_456_789,
                                         tau_ns=800.0)),
+    "source_outside_crystal": (BOX_CSI, OP_C1, Readout(GRID), TB80,
+                               dict(n_photons=20_000, seed=5, positions=[(-3.0, 24.0, 10.0),
+                                                                          (24.0, 60.0, 40.0)],
+                                    tau_ns=TAU_C1)),
     "cap_and_overflow": (BOX_CSI, ideal(1.95), Readout(GRID), TimeBinning(1.0, 3),
                          dict(n_photons=20_000, seed=2, pos=CENTRE_CSI, tau_ns=0.0,
                               max_bounces=50)),
