@@ -42,6 +42,102 @@ import numpy as np
 # instrumented oracle (python -m oracle.opcount).
 OPS_PER_STEP = {"scan256": 165.6, "point1m": 186.7}
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) per launch of the transport kernel from ncu
+# (profiles/transport_kernel_*.md); independent of the photon count: the only
+# DRAM traffic is the sources, offsets and output maps.
+TRAFFIC_BYTES = {"scan256": 218_624, "point1m": 82_944}
+
+
+def events_workload(n_events: int = 50_000):
+    """Config 3: 511 keV gammas on CsI(Tl) + Teflon (runs/gammas_csitl_50k.toml:
+    seed 11, PDE 0.40, 100 ns x 80 bins, yield 54000/MeV, tau 1000 ns)."""
+    from crysplight_b200.params import (Box, OpticalParams, Readout, SipmGrid, TimeBinning,
+                                        deg2rad_f32)
+    from crysplight_b200.events import GammaMaterial
+    box = Box((48.0, 48.0, 37.2))
+    op = OpticalParams(1.79, 1.45, 3115.0, 346.0, 0.99, False, True, deg2rad_f32(1.3), 0.40)
+    return dict(name="events_csitl", box=box, op=op, ro=Readout(SipmGrid(6.0, 8, 8)),
+                tb=TimeBinning(100.0, 80), tau=1000.0, seed=11, yield_=54_000.0,
+                mat=GammaMaterial.from_csv("CsI", 4.51, "xcom_CSI.csv"), n_events=n_events,
+                desc=f"{n_events} 511 keV gammas, CsI(Tl)+Teflon 48x48x37.2 mm, PDE 0.40")
+
+
+def run_events_bench(eng, E, steps: int, warmup: int, dev, stream, pid_base: int = 0):
+    """events/s: transport of all events' photons with the deposits in HBM
+    (value), and the whole public pipeline run_events (e2e)."""
+    import torch
+    from crysplight_b200.events import gamma_stage, run_events
+    g = gamma_stage(E["mat"], E["box"], n_events=E["n_events"], seed=E["seed"],
+                    yield_per_mev=E["yield_"])
+    nd = g.dep_photons.size
+    off = np.zeros(nd + 1, np.int64)
+    np.cumsum(g.dep_photons, out=off[1:])
+    d = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in
+         dict(x=g.dep_xyz[:, 0], y=g.dep_xyz[:, 1], z=g.dep_xyz[:, 2], t=g.dep_t, off=off,
+              seg=g.dep_event).items()}
+    n_seg = E["n_events"]
+    maps = torch.empty(64 * n_seg, dtype=torch.int32, device=dev)
+    tmin = torch.empty(64 * n_seg, dtype=torch.float32, device=dev)
+    npe = torch.empty(n_seg, dtype=torch.int32, device=dev)
+    ctr = torch.empty(9, dtype=torch.int64, device=dev)
+    sptr = stream.cuda_stream
+
+    def step():
+        eng.run_segments_device(E["box"], E["op"], E["ro"], E["tb"], sx=d["x"].data_ptr(),
+                                sy=d["y"].data_ptr(), sz=d["z"].data_ptr(), st=d["t"].data_ptr(),
+                                src_offsets=d["off"].data_ptr(), src_segment=d["seg"].data_ptr(),
+                                n_src=nd, n_segments=n_seg, n_photons=int(off[-1]),
+                                seed=E["seed"], pid_offset=pid_base, tau_ns=E["tau"],
+                                maps=maps.data_ptr(), tmin=tmin.data_ptr(), npe=npe.data_ptr(),
+                                counters=ctr.data_ptr(), stream=sptr)
+    for _ in range(warmup):
+        step()
+    eng.sync(sptr)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    for a, b in ev:
+        flush.zero_()
+        a.record(stream)
+        step()
+        b.record(stream)
+    eng.sync(sptr)
+    torch.cuda.synchronize(dev)
+    dev_s = sum(a.elapsed_time(b) for a, b in ev) * 1e-3 / steps
+    photon_steps = eng.last_steps
+    run_events(E["box"], E["op"], E["ro"], E["tb"], E["mat"], E["yield_"],
+               n_events=E["n_events"], seed=E["seed"], tau_ns=E["tau"], engine=eng)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        run_events(E["box"], E["op"], E["ro"], E["tb"], E["mat"], E["yield_"],
+                   n_events=E["n_events"], seed=E["seed"], tau_ns=E["tau"], engine=eng)
+    e2e_s = (time.perf_counter() - t0) / steps
+    return dict(value=E["n_events"] / dev_s, e2e=E["n_events"] / e2e_s, dev_s=dev_s,
+                e2e_s=e2e_s, photons=int(off[-1]), photon_steps=photon_steps, deposits=nd,
+                h2d=int(3 * 4 * nd + 4 * nd + 8 * (nd + 1) + 4 * nd),
+                d2h=int(2 * 4 * 64 * n_seg + 4 * n_seg + 72 + 12))
+
+
+def events_cpu_baseline(E, target_s: float) -> dict:
+    """The oracle transports the photons of a sample of events (after the host
+    gamma stage) on all host threads: events/s."""
+    from oracle import oracle
+    from crysplight_b200.events import gamma_stage
+    n = 50
+    while True:
+        g = gamma_stage(E["mat"], E["box"], n_events=n, seed=E["seed"], yield_per_mev=E["yield_"])
+        t0 = time.perf_counter()
+        oracle.run_segments(E["box"], E["op"], E["ro"], E["tb"], sources=g.dep_xyz,
+                            photons_per_source=g.dep_photons, segment_of_source=g.dep_event,
+                            n_segments=n, seed=E["seed"], t0s=g.dep_t, tau_ns=E["tau"],
+                            nthreads=os.cpu_count())
+        dt = time.perf_counter() - t0
+        if dt > 0.3 * target_s or n >= E["n_events"]:
+            break
+        n = min(E["n_events"], int(n * max(2.0, target_s / max(dt, 1e-3))))
+    return {"value": n / dt, "unit": "events/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"first {n} of the {E['n_events']} events ({dt:.1f} s on "
+                      f"{os.cpu_count()} threads; gamma stage excluded)"}
 
 
 def workload(name: str, points: int = 256, per_point: int = 200_000):
@@ -346,7 +442,7 @@ def run_cuda_arm(args, W, rank, world, local_rank):
         "photon_steps_per_s": steps_per_launch / launch_s,
         "roofline": {
             "bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gop/s",
-            "frac": achieved / peak, "traffic": None,
+            "frac": achieved / peak, "traffic": TRAFFIC_BYTES.get(W["name"]),
             "ops_per_step": ops_step,
             "note": ("reference Float32/int ops per photon-step x steps / launch time, against "
                      "one op per lane per clock (SMs x 128 lanes x max SM clock of measured)"),
@@ -358,7 +454,73 @@ def run_cuda_arm(args, W, rank, world, local_rank):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(W, args.cpu_seconds)
+    if world == 1 and args.events > 0:
+        # secondary metric: 511 keV events/s of the event pipeline (config 3 sample)
+        E = events_workload(args.events)
+        r = run_events_bench(eng, E, args.steps, args.warmup, dev, stream)
+        line["events"] = {"metric": "511keV events/s", "workload": E["desc"],
+                          "value": r["value"], "e2e": r["e2e"], "unit": "events/s",
+                          "photons_per_event": r["photons"] / E["n_events"],
+                          "photon_steps_per_s": r["photon_steps"] / r["dev_s"]}
     print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def run_events_arm(args, rank, world, local_rank):
+    """--workload events_csitl: events/s of the 511 keV event pipeline."""
+    import torch
+    import crysplight_b200 as cl
+    if rank != 0 and args.impl == "reference":
+        return
+    E = events_workload(args.n_events)
+    if args.impl == "reference":
+        base = events_cpu_baseline(E, args.cpu_seconds)
+        for _ in range(args.warmup):
+            pass
+        line = {"impl": "reference", "metric": "511keV events/s", "value": base["value"],
+                "unit": "events/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 / base["value"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": E["name"], "desc": E["desc"]}, "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": "events/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    eng = cl.Engine(local_rank)
+    r = run_events_bench(eng, E, args.steps, args.warmup, dev, stream, pid_base=0)
+    dev_s, e2e_s = r["dev_s"], r["e2e_s"]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s, e2e_s = float(t[0]), float(t[1])
+    if rank == 0:
+        peaks = measured_peaks()
+        n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+        ops = OPS_PER_STEP["point1m"]
+        achieved = ops * r["photon_steps"] / dev_s
+        peak = n_sm * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6
+        line = {"metric": "511keV events/s", "value": world * E["n_events"] / dev_s,
+                "unit": "events/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": dev_s * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": E["name"], "desc": E["desc"],
+                           "photons_per_step": r["photons"], "deposits": r["deposits"],
+                           "l2": "flushed between timed steps (256 MiB memset)"},
+                "e2e": {"value": world * E["n_events"] / e2e_s, "unit": "events/s",
+                        "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+                "gpu_launches": 3 * args.steps,
+                "photon_steps_per_launch": r["photon_steps"],
+                "roofline": {"bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9,
+                             "unit": "Gop/s", "frac": achieved / peak, "traffic": None,
+                             "ops_per_step": ops}}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = events_cpu_baseline(E, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
     eng.close()
 
 
@@ -368,7 +530,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
-    ap.add_argument("--workload", choices=("scan256", "point1m"), default="scan256")
+    ap.add_argument("--workload", choices=("scan256", "point1m", "events_csitl"),
+                    default="scan256")
+    ap.add_argument("--events", type=int, default=10_000,
+                    help="events in the secondary events/s measurement of the default run "
+                         "(0 = skip)")
+    ap.add_argument("--n-events", type=int, default=50_000,
+                    help="events of --workload events_csitl")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=256,
@@ -380,6 +548,20 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "events_csitl":
+        if world > 1 and args.impl == "cuda":
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        try:
+            run_events_arm(args, rank, world, local_rank)
+        finally:
+            if world > 1 and args.impl == "cuda":
+                import torch.distributed as dist
+                dist.destroy_process_group()
+        return
     W = workload(args.workload, args.points, args.photons_per_point)
     if args.impl == "reference":
         run_reference_arm(args, W, rank, world)

@@ -263,6 +263,58 @@ int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta,
 int cl_debug_eval(cl_handle* h, int fn, const void* in, void* out, int64_t n,
                   uint64_t seed, int32_t n_per);
 
+/* ---------------------------------------------------------------------------
+ * Host-side 511 keV gamma stage of the event pipeline (no GPU involved).
+ * The reference runs it in Julia (its vendored gamma core, src/gamma/*.jl,
+ * through src/gamma_interface.jl); these restate it in C.  Each event draws
+ * from its own Philox4x32-10 stream keyed by (seed, event number), so the
+ * gamma stage is statistically, not bitwise, equivalent to the reference
+ * (whose Julia Xoshiro stream cannot be reproduced here).
+ * ------------------------------------------------------------------------- */
+typedef struct cl_gamma_material cl_gamma_material;
+
+/* make_material(name, density, xcom_csv) (src/gamma/gmaterials.jl:22-31):
+ * XCOM columns in cm^2/g at n energies (MeV, duplicate K-edge energies
+ * allowed), density in g/cm^3.  n = 0 gives the vacuum material. */
+int cl_gamma_material_create(cl_gamma_material** out, const double* E_MeV,
+                             const double* incoherent, const double* photoelectric,
+                             const double* pair_nuclear, const double* pair_electron,
+                             int32_t n, double density);
+void cl_gamma_material_destroy(cl_gamma_material* m);
+const char* cl_gamma_last_error(void);
+
+/* sigma_macro (src/gamma/gmaterials.jl:45-57): sigma3 = (Compton,
+ * photoelectric, pair) macroscopic cross sections in 1/cm at E_MeV. */
+int cl_gamma_sigma(const cl_gamma_material* m, double E_MeV, double* sigma3);
+
+/* gamma_deposits (src/gamma_interface.jl:30-49) for one gamma entering the
+ * crystal at entry_mm along dir, drawing from stream `stream` of `seed`:
+ * dep6[6*i..] = (x, y, z [mm], E [keV], t [ns], process 0 photo / 1 Compton /
+ * 2 below the 10 keV cut). */
+int cl_gamma_deposits(const cl_gamma_material* m, const cl_box* box, const float* entry_mm,
+                      const double* dir, double e0_mev, uint64_t seed, uint64_t stream,
+                      float* dep6, int32_t max_dep, int32_t* n_dep);
+
+/* rand_poisson (src/events.jl:11-22) drawing from stream `stream` of `seed`. */
+int64_t cl_rand_poisson(uint64_t seed, uint64_t stream, double lam);
+
+/*
+ * The gamma half of run_events! (src/events.jl:93-118) for events
+ * ev0+1 .. ev0+n_events (1-based event numbers key the streams): per event
+ * the entry point uniform on z = 0, the deposits, the truth record (edep,
+ * xyz1[3], e1, xyz2[3], e2, er [keV / mm], int_type, n_int) and, per deposit
+ * in event order, its position, time, event index (0-based within the call)
+ * and Poisson photon count for yield_per_mev.  Deposits beyond max_deposits
+ * give CL_ERR_ARG with *n_deposits set to the number needed.  nthreads <= 0
+ * uses every hardware thread; results do not depend on it.
+ */
+int cl_gamma_events(const cl_gamma_material* m, const cl_box* box, int64_t ev0,
+                    int64_t n_events, uint64_t seed, double e0_mev, double yield_per_mev,
+                    int nthreads, float* edep, float* xyz1, float* e1, float* xyz2,
+                    float* e2, float* er, int8_t* int_type, int16_t* n_int,
+                    int64_t max_deposits, float* dep_xyz, float* dep_t,
+                    int32_t* dep_event, int64_t* dep_photons, int64_t* n_deposits);
+
 /*
  * Allocation-free point-source transport.  No counterpart in the reference:
  * it exists for callers that cannot let a library call cudaMalloc — programs
