@@ -263,6 +263,16 @@ int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta,
 int cl_debug_eval(cl_handle* h, int fn, const void* in, void* out, int64_t n,
                   uint64_t seed, int32_t n_per);
 
+/*
+ * Diagnostic for tests: C = A * B^T on the tcgen05 tensor cores, A [M][K] and
+ * B [N][K] BF16 row-major device arrays, C [M][N] FP32 device (or, with
+ * splits > 1, K-split partials C[split][M][N]).  M % 128 == 0, N % 32 == 0,
+ * N <= 256, K % 64 == 0.  *d_err (device) gets bit 0 set if a completion wait
+ * ran out.  Enqueued on `stream`; no synchronisation.
+ */
+int cl_umma_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K,
+                      int grid_x, int splits, unsigned int* d_err, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Host-side 511 keV gamma stage of the event pipeline (no GPU involved).
  * The reference runs it in Julia (its vendored gamma core, src/gamma/*.jl,
