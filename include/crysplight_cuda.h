@@ -274,6 +274,41 @@ int cl_umma_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int 
                       int grid_x, int splits, unsigned int* d_err, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Light-response surrogate network (no counterpart in the reference, which
+ * always runs the Monte Carlo): a 3 -> 256 -> 256 -> 256 -> 192 SiLU MLP
+ * trained and evaluated on the tcgen05 tensor cores (BF16 weights and
+ * activations, FP32 accumulation, Adam on FP32 master weights).  Parameters
+ * are one FP32 block of cl_mlp_param_count() floats:
+ * W1[256][3] b1[256] W2[256][256] b2[256] W3[256][256] b3[256] W4[192][256] b4[192]
+ * (W[out][in]).  A cl_mlp owns one stream and is not re-entrant.
+ * ------------------------------------------------------------------------- */
+typedef struct cl_mlp cl_mlp;
+
+int cl_mlp_param_count(void);
+/* max_batch % 128 == 0; parameters start at zero (set them before use). */
+int cl_mlp_create(cl_mlp** out, int device, int max_batch);
+void cl_mlp_destroy(cl_mlp* m);
+const char* cl_mlp_last_error(const cl_mlp* m);
+/* Host buffers of cl_mlp_param_count() floats; setting resets Adam's state. */
+int cl_mlp_set_params(cl_mlp* m, const float* host);
+int cl_mlp_get_params(cl_mlp* m, float* host);
+/* Training set x [n][3], targets t [n][192]: FP32 device arrays owned by the
+ * caller, alive across the cl_mlp_train calls. */
+int cl_mlp_set_data(cl_mlp* m, const float* d_x, const float* d_t, int64_t n);
+/* `steps` Adam steps (lr, betas 0.9/0.999) on minibatches of `batch` rows
+ * (batch % 128 == 0, <= max_batch) drawn with replacement by Philox from
+ * (seed, step0 + s); loss = mean squared error over all 192 outputs.
+ * *loss_out = mean loss over the steps. */
+int cl_mlp_train(cl_mlp* m, int steps, int batch, float lr, uint32_t seed, uint32_t step0,
+                 float* loss_out);
+/* Inference: out [n][192] FP32 device for x [n][3] FP32 device. */
+int cl_mlp_forward(cl_mlp* m, const float* d_x, float* d_out, int64_t n);
+/* Loss and gradient (host, cl_mlp_param_count() floats) for one batch of
+ * B rows (B % 128 == 0, <= max_batch), without an update.  For tests. */
+int cl_mlp_gradient(cl_mlp* m, const float* d_x, const float* d_t, int B, float* host_grad,
+                    float* loss_out);
+
+/* ---------------------------------------------------------------------------
  * Host-side 511 keV gamma stage of the event pipeline (no GPU involved).
  * The reference runs it in Julia (its vendored gamma core, src/gamma/*.jl,
  * through src/gamma_interface.jl); these restate it in C.  Each event draws
