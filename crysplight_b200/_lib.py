@@ -20,8 +20,13 @@ EXPORTS = (
     "cl_version", "cl_abi_version", "cl_create", "cl_destroy", "cl_last_error",
     "cl_run_photons", "cl_run_photons_device", "cl_run_segments",
     "cl_run_segments_device", "cl_sync", "cl_last_steps", "cl_set_launch",
-    "cl_debug_eval", "cl_run_photons_noalloc",
+    "cl_debug_eval", "cl_run_photons_noalloc", "cl_run_segments_moments_device",
 )
+
+# Fixed-point scales of cl_run_segments_moments_device (crysplight_cuda.h)
+MOMENT_T_SCALE = 1048576.0
+MOMENT_T2_SCALE = 65536.0
+MOMENT_T_MAX_NS = 4096.0
 
 CL_OK = 0
 CL_ERR_ARG = -1
@@ -75,6 +80,10 @@ def _declare(lib: C.CDLL) -> None:
         _P, _P, _P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int64, C.c_uint64, C.c_uint64, C.c_float,
         C.c_int32, _P, _P, _P, _P, C.POINTER(Records), _P]
     lib.cl_run_segments_device.restype = C.c_int
+    lib.cl_run_segments_moments_device.argtypes = common + [
+        _P, _P, _P, _P, _P, _P, C.c_int64, C.c_int64, C.c_int64, C.c_uint64, C.c_uint64, C.c_float,
+        C.c_int32, _P, _P, _P, _P, _P, _P, _P]
+    lib.cl_run_segments_moments_device.restype = C.c_int
     lib.cl_sync.argtypes = [_P, _P]
     lib.cl_sync.restype = C.c_int
     lib.cl_last_steps.argtypes = [_P]

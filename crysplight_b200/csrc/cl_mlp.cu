@@ -1,13 +1,13 @@
 // cl_mlp.cu — the light-response surrogate: a 3 -> 256 -> 256 -> 256 -> 192 SiLU
 // MLP trained and evaluated on sm_100a by hand-written kernels.
 //
-// GEMMs run on the 5th-generation tensor cores: BF16 operands staged in shared
-// memory (canonical K-major layout, see cl_umma.cuh), one thread issuing
-// tcgen05.mma with the FP32 accumulator in tensor memory, completion through
-// tcgen05.commit on an mbarrier (bounded wait), and epilogues fused on the
-// TMEM -> register path (bias, SiLU, SiLU', BF16 casts, transposed copies,
-// split-K partials).  The 3-wide input layer, the loss, the reductions and
-// Adam run on the CUDA cores.
+// GEMMs run on the 5th-generation tensor cores: BF16 operands streamed by TMA
+// into a 4-stage shared-memory ring (128-byte swizzled K-major tiles), one
+// thread issuing tcgen05.mma into a double-buffered FP32 accumulator in tensor
+// memory, and four warps draining it through fused epilogues (bias, SiLU,
+// SiLU', the loss and its gradient, bias-gradient column sums, the layer-1
+// gradients, BF16 casts, transposed copies, split-K partials).  The 3-wide
+// input layer, the split-K reduction and Adam run on the CUDA cores.
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -15,6 +15,10 @@
 #include <new>
 #include <vector>
 
+#include <mutex>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -27,23 +31,32 @@ namespace mlp {
 using bf16 = __nv_bfloat16;
 
 constexpr int TILE_M = 128;     // rows per CTA tile (TMEM lanes)
-constexpr int TILE_K = 64;      // K elements staged per chunk
-constexpr int GEMM_THREADS = 128;
+constexpr int TILE_K = 64;      // K elements per pipeline stage (one 128-byte swizzle row)
+constexpr int STAGES = 4;       // TMA -> MMA pipeline depth
+constexpr int EPI_WARPS = 4;    // warps 0-3: epilogue (TMEM lane quadrants 0-3)
+constexpr int GEMM_THREADS = 192;   // + warp 4: TMA producer, warp 5: MMA issuer / TMEM owner
+constexpr uint32_t TMEM_COLS = 512; // two 256-column FP32 accumulators
 constexpr uint32_t WAIT_BUDGET = 1u << 22;   // polls before a wait gives up
-constexpr size_t GEMM_SMEM_BYTES = 100 * 1024;
+constexpr int RED_STRIDE = 33;
+constexpr size_t RED_BYTES = (size_t)EPI_WARPS * (32 * RED_STRIDE + 32 * 3) * sizeof(float);
+
+__host__ __device__ constexpr size_t gemm_smem_bytes(int N)
+{
+    return 1024 + (size_t)STAGES * ((size_t)TILE_M * 128 + (size_t)N * 128) + RED_BYTES;
+}
 
 enum Epi : int {
     EPI_F32 = 0,         // out_f[m][n] = acc
     EPI_BIAS_SILU = 1,   // z = acc + b: out_z = bf16(z), out_h = bf16(silu z), out_ht = transposed
     EPI_BIAS_F32 = 2,    // out_f[m][n] = acc + b
-    EPI_DSILU = 3,       // d = acc * silu'(zprev): out_h = bf16(d), out_ht = transposed
+    EPI_DSILU = 3,       // g = bf16(acc * silu'(zprev)): out_h, out_ht, colsum += column sums of g
     EPI_PARTIAL = 4,     // out_f[split][m][n] = acc (split-K partial)
+    EPI_LOSS = 5,        // o = acc + b, d = o - target: loss += scale d^2, g = bf16(2 scale d) -> out_h, out_ht, colsum
+    EPI_DSILU_L1 = 6,    // as EPI_DSILU with zprev recomputed from x, W1, b1; colsum and gw1 += g, g x
 };
 
 struct GemmArgs {
-    const bf16* A; int64_t lda;     // [M][K], K-major
-    const bf16* B; int64_t ldb;     // [N][K], K-major
-    int M, N, K;                    // M % 128 == 0, N % 32 == 0 && N <= 256, K % 64 == 0
+    int M, N, K;                    // M % 128 == 0, N % 32 == 0 && 32 <= N <= 256, K % 64 == 0
     int k_split;                    // K elements per split (gridDim.y splits)
     const float* bias;
     float* out_f; int64_t ldf;
@@ -51,6 +64,11 @@ struct GemmArgs {
     bf16* out_ht; int64_t ldht;     // [N][M]
     bf16* out_z;                    // [M][N], ld = ldh
     const bf16* zprev;              // [M][N], ld = ldh
+    const float* target;            // EPI_LOSS: [M][N] FP32
+    float scale;
+    float* loss;
+    float* colsum;                  // [N]
+    const float* x; const float* w1; float* gw1;   // EPI_DSILU_L1: x [M][3], W1 [N][3], grad W1 [N][3]
     unsigned int* err;
 };
 
@@ -61,149 +79,302 @@ __device__ __forceinline__ float dsilu(float z)
     return s * (1.0f + z * (1.0f - s));
 }
 
-// Stage rows [r0, r0+R) x K-chunk [k0, k0+64) of a K-major matrix into the
-// canonical layout (16-byte pieces, 8 consecutive threads per row).
-__device__ __forceinline__ void stage_tile(uint8_t* smem, const bf16* g, int64_t ld, int r0, int R,
-                                           int k0)
+// Column sums over the warp's 32 rows of g[32] (one row per lane), added to
+// dst[0..31]; with xs (the rows' inputs), also sum g x_k added to gw[c*3 + k].
+__device__ __forceinline__ void warp_col_sums(float* red, const float* g, int lane, float* dst,
+                                              const float* xs, float* gw)
 {
-    const int pieces = R * (TILE_K / 8);
-    for (int p = threadIdx.x; p < pieces; p += blockDim.x) {
-        const int r = p >> 3, c = p & 7;
-        const uint4 v = *reinterpret_cast<const uint4*>(g + (int64_t)(r0 + r) * ld + k0 + 8 * c);
-        *reinterpret_cast<uint4*>(smem + umma::tile_offset((uint32_t)r, (uint32_t)(8 * c), (uint32_t)R)) = v;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) red[lane * RED_STRIDE + i] = g[i];
+    __syncwarp();
+    float s = 0.0f, s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+#pragma unroll 8
+    for (int r = 0; r < 32; ++r) {
+        const float v = red[r * RED_STRIDE + lane];
+        s += v;
+        if (xs) { s0 += v * xs[r * 3]; s1 += v * xs[r * 3 + 1]; s2 += v * xs[r * 3 + 2]; }
+    }
+    atomicAdd(dst + lane, s);
+    if (xs) {
+        atomicAdd(gw + lane * 3, s0);
+        atomicAdd(gw + lane * 3 + 1, s1);
+        atomicAdd(gw + lane * 3 + 2, s2);
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void store_row_bf16(bf16* dst, const bf16* h)
+{
+    uint4* d = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d[i] = reinterpret_cast<const uint4*>(h)[i];
+}
+
+// Epilogue of one 128 x N tile: warp w owns rows row0 + 32w + lane.
+template <int EPI>
+__device__ __forceinline__ void epilogue(const GemmArgs& G, uint32_t tbase, int row, float* red, int lane)
+{
+    const int N = G.N;
+    float sq = 0.0f;
+    float* xs = red + 32 * RED_STRIDE;
+    float x0 = 0.f, x1 = 0.f, x2 = 0.f;
+    if (EPI == EPI_DSILU_L1) {
+        x0 = G.x[(int64_t)row * 3]; x1 = G.x[(int64_t)row * 3 + 1]; x2 = G.x[(int64_t)row * 3 + 2];
+        xs[lane * 3] = x0; xs[lane * 3 + 1] = x1; xs[lane * 3 + 2] = x2;
+        __syncwarp();
+    }
+    for (int c0 = 0; c0 < N; c0 += 32) {
+        float v[32];
+        umma::tmem_ld32(tbase + (uint32_t)c0, v);
+        if (EPI == EPI_F32 || EPI == EPI_BIAS_F32 || EPI == EPI_PARTIAL) {
+            float* o = G.out_f + (EPI == EPI_PARTIAL ? (int64_t)blockIdx.y * G.M * G.ldf : 0) +
+                       (int64_t)row * G.ldf + c0;
+#pragma unroll
+            for (int i = 0; i < 32; i += 4) {
+                float4 q;
+                q.x = v[i] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i] : 0.0f);
+                q.y = v[i + 1] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i + 1] : 0.0f);
+                q.z = v[i + 2] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i + 2] : 0.0f);
+                q.w = v[i + 3] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i + 3] : 0.0f);
+                *reinterpret_cast<float4*>(o + i) = q;
+            }
+        } else if (EPI == EPI_BIAS_SILU) {
+            __align__(16) bf16 h[32];
+            __align__(16) bf16 zz[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const float z = v[i] + G.bias[c0 + i];
+                zz[i] = __float2bfloat16_rn(z);
+                h[i] = __float2bfloat16_rn(silu(z));
+                if (G.out_ht) G.out_ht[(int64_t)(c0 + i) * G.ldht + row] = h[i];
+            }
+            store_row_bf16(G.out_h + (int64_t)row * G.ldh + c0, h);
+            if (G.out_z) store_row_bf16(G.out_z + (int64_t)row * G.ldh + c0, zz);
+        } else {   // EPI_LOSS, EPI_DSILU, EPI_DSILU_L1: a BF16 gradient and its column sums
+            __align__(16) bf16 h[32];
+            float gf[32];
+            if (EPI == EPI_LOSS) {
+                const float4* t4 = reinterpret_cast<const float4*>(G.target + (int64_t)row * N + c0);
+#pragma unroll
+                for (int i = 0; i < 32; i += 4) {
+                    const float4 t = t4[i / 4];
+                    const float tt[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float d = (v[i + q] + G.bias[c0 + i + q]) - tt[q];
+                        sq += d * d;
+                        h[i + q] = __float2bfloat16_rn(2.0f * d * G.scale);
+                    }
+                }
+            } else if (EPI == EPI_DSILU) {
+                __align__(16) bf16 zp[32];
+                const uint4* z4 = reinterpret_cast<const uint4*>(G.zprev + (int64_t)row * G.ldh + c0);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) reinterpret_cast<uint4*>(zp)[i] = z4[i];
+#pragma unroll
+                for (int i = 0; i < 32; ++i) h[i] = __float2bfloat16_rn(v[i] * dsilu(__bfloat162float(zp[i])));
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const int c = c0 + i;
+                    // the forward's pre-activation, same operations in the same order
+                    const float z = G.bias[c] + x0 * G.w1[c * 3] + x1 * G.w1[c * 3 + 1] + x2 * G.w1[c * 3 + 2];
+                    const float zq = __bfloat162float(__float2bfloat16_rn(z));
+                    h[i] = __float2bfloat16_rn(v[i] * dsilu(zq));
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                gf[i] = __bfloat162float(h[i]);
+                if (EPI != EPI_DSILU_L1 && G.out_ht) G.out_ht[(int64_t)(c0 + i) * G.ldht + row] = h[i];
+            }
+            if (EPI != EPI_DSILU_L1 && G.out_h) store_row_bf16(G.out_h + (int64_t)row * G.ldh + c0, h);
+            warp_col_sums(red, gf, lane, G.colsum + c0, EPI == EPI_DSILU_L1 ? xs : nullptr,
+                          EPI == EPI_DSILU_L1 ? G.gw1 + (int64_t)c0 * 3 : nullptr);
+        }
+    }
+    if (EPI == EPI_LOSS) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        if (lane == 0) atomicAdd(G.loss, sq * G.scale);
     }
 }
 
+// C = A B^T on the tensor cores.  A [M][K] and B [N][K] BF16, K-major, read
+// through TMA tensor maps (128-byte swizzle, boxes of 64 x 128 rows and 64 x N
+// rows).  Persistent over 128-row tiles (blockIdx.x, stride gridDim.x), K split
+// over blockIdx.y.  Roles: warp 4 lane 0 streams A/B stages (full/empty
+// mbarriers), warp 5 lane 0 issues tcgen05.mma into one of two TMEM
+// accumulators and commits, warps 0-3 drain the other accumulator through the
+// epilogue.  Every wait is bounded; a wait that runs out sets bit 0 of *err,
+// tells the other roles to stop, and the CTA still waits (bounded) for its
+// copies and MMAs in flight before freeing TMEM.
 template <int EPI>
-__global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(const __grid_constant__ GemmArgs G)
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
+    gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                const __grid_constant__ GemmArgs G)
 {
-    extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* sA = smem;                                  // 128 x 64 bf16 = 16 KB
-    uint8_t* sB = smem + TILE_M * TILE_K * 2;            // N x 64 bf16 <= 32 KB
-    __shared__ __align__(8) uint64_t mbar;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    const int N = G.N;
+    const uint32_t a_bytes = TILE_M * 128, stage_bytes = a_bytes + (uint32_t)N * 128;
+    float* red_all = reinterpret_cast<float*>(smem + STAGES * stage_bytes);
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
 
+    const int split = blockIdx.y;
+    const int k_begin = split * G.k_split;
+    const int k_end = min(G.K, k_begin + G.k_split);
+    const int n_chunks = (k_end - k_begin) / TILE_K;
+    const int n_tiles = G.M / TILE_M;
+    if (n_chunks <= 0 || (int)blockIdx.x >= n_tiles) return;   // uniform over the CTA
+
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int N = G.N;
-    if (warp == 0) umma::tmem_alloc(&tmem_slot, 256);
+    volatile int* abort_v = &abort_flag;
     if (threadIdx.x == 0) {
-        umma::mbar_init(&mbar, 1);
+        for (int s = 0; s < STAGES; ++s) { umma::mbar_init(&full[s], 1); umma::mbar_init(&empty[s], 1); }
+        for (int a = 0; a < 2; ++a) { umma::mbar_init(&acc_full[a], 1); umma::mbar_init(&acc_empty[a], EPI_WARPS); }
         abort_flag = 0;
     }
+    if (warp == 5) umma::tmem_alloc(&tmem_slot, TMEM_COLS);
+    if (warp == 4 && lane == 0) { umma::prefetch_tmap(&tmA); umma::prefetch_tmap(&tmB); }
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-    const uint32_t idesc = umma::make_idesc_bf16(TILE_M, N);
-    const uint32_t lbo_a = (TILE_M / 8) * 128, lbo_b = (uint32_t)(N / 8) * 128;
-    const uint32_t sa = umma::smem_u32(sA), sb = umma::smem_u32(sB);
-    uint32_t phase = 0;
 
-    const int k_begin = blockIdx.y * G.k_split;
-    const int k_end = min(G.K, k_begin + G.k_split);
-    const int n_tiles = G.M / TILE_M;
-    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        const int m0 = tile * TILE_M;
-        for (int k0 = k_begin; k0 < k_end; k0 += TILE_K) {
-            stage_tile(sA, G.A, G.lda, m0, TILE_M, k0);
-            stage_tile(sB, G.B, G.ldb, 0, N, k0);
-            umma::fence_async_smem();
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                umma::fence_after_sync();
-#pragma unroll
-                for (int s = 0; s < TILE_K / 16; ++s) {
-                    const uint64_t ad = umma::make_desc(sa + 2 * s * lbo_a, lbo_a, 128);
-                    const uint64_t bd = umma::make_desc(sb + 2 * s * lbo_b, lbo_b, 128);
-                    umma::mma_bf16(tmem, ad, bd, idesc, (k0 > k_begin || s > 0) ? 1u : 0u);
-                }
-                umma::commit(&mbar);
-            }
-            if (!umma::mbar_wait(&mbar, phase, WAIT_BUDGET)) {
-                atomicOr(G.err, 1u);
-                abort_flag = 1;
-            }
-            phase ^= 1u;
-            __syncthreads();
-            if (abort_flag) break;
-        }
-        if (abort_flag) break;
-
-        // ---- epilogue: warp w owns rows m0 + 32w + lane ----
-        umma::fence_after_sync();
-        const int row = m0 + 32 * warp + lane;
-        for (int c0 = 0; c0 < N; c0 += 32) {
-            float v[32];
-            umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
-            if (EPI == EPI_F32 || EPI == EPI_BIAS_F32 || EPI == EPI_PARTIAL) {
-                float* o = G.out_f + (EPI == EPI_PARTIAL ? (int64_t)blockIdx.y * G.M * G.ldf : 0) +
-                           (int64_t)row * G.ldf + c0;
-#pragma unroll
-                for (int i = 0; i < 32; i += 4) {
-                    float4 q;
-                    q.x = v[i] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i] : 0.0f);
-                    q.y = v[i + 1] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i + 1] : 0.0f);
-                    q.z = v[i + 2] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i + 2] : 0.0f);
-                    q.w = v[i + 3] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i + 3] : 0.0f);
-                    *reinterpret_cast<float4*>(o + i) = q;
-                }
-            } else {
-                __align__(16) bf16 h[32];
-                __align__(16) bf16 zz[32];
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    float r;
-                    if (EPI == EPI_BIAS_SILU) {
-                        const float z = v[i] + G.bias[c0 + i];
-                        zz[i] = __float2bfloat16_rn(z);
-                        r = silu(z);
-                    } else {   // EPI_DSILU
-                        const float zp = __bfloat162float(G.zprev[(int64_t)row * G.ldh + c0 + i]);
-                        r = v[i] * dsilu(zp);
+    if (warp == 4) {
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+                for (int c = 0; c < n_chunks; ++c, ++it) {
+                    const uint32_t s = it % STAGES, r = it / STAGES;
+                    if (r > 0 && !umma::mbar_wait_or_abort(&empty[s], (r - 1) & 1u, WAIT_BUDGET, abort_v)) {
+                        ok = false;
+                        break;
                     }
-                    h[i] = __float2bfloat16_rn(r);
-                    if (G.out_ht) G.out_ht[(int64_t)(c0 + i) * G.ldht + row] = h[i];
-                }
-                uint4* dst = reinterpret_cast<uint4*>(G.out_h + (int64_t)row * G.ldh + c0);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) dst[i] = reinterpret_cast<const uint4*>(h)[i];
-                if (EPI == EPI_BIAS_SILU && G.out_z) {
-                    uint4* dz = reinterpret_cast<uint4*>(G.out_z + (int64_t)row * G.ldh + c0);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) dz[i] = reinterpret_cast<const uint4*>(zz)[i];
+                    uint8_t* st = smem + s * stage_bytes;
+                    umma::mbar_arrive_expect_tx(&full[s], stage_bytes);
+                    umma::tma_load_2d(st, &tmA, k_begin + c * TILE_K, tile * TILE_M, &full[s]);
+                    umma::tma_load_2d(st + a_bytes, &tmB, k_begin + c * TILE_K, 0, &full[s]);
                 }
             }
+            if (!ok) { atomicOr(G.err, 1u); *abort_v = 1; }
+            // copies still in flight land before the CTA can exit
+            for (uint32_t j = it > (uint32_t)STAGES ? it - STAGES : 0u; j < it; ++j)
+                umma::mbar_wait(&full[j % STAGES], (j / STAGES) & 1u, WAIT_BUDGET);
         }
-        umma::fence_before_sync();
-        __syncthreads();          // TMEM reads done before the next tile overwrites it
-    }
-    if (abort_flag) {
-        // give in-flight MMAs one more bounded chance to land before freeing TMEM
-        umma::mbar_wait(&mbar, phase, WAIT_BUDGET);
+    } else if (warp == 5) {
+        if (lane == 0) {
+            const uint32_t idesc = umma::make_idesc_bf16(TILE_M, N);
+            uint32_t it = 0, j = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++j) {
+                const uint32_t a = j & 1u, u = j >> 1;
+                if (u > 0 && !umma::mbar_wait_or_abort(&acc_empty[a], (u - 1) & 1u, WAIT_BUDGET, abort_v)) {
+                    ok = false;
+                    break;
+                }
+                umma::fence_after_sync();
+                const uint32_t d = tmem + a * 256u;
+                for (int c = 0; c < n_chunks; ++c, ++it) {
+                    const uint32_t s = it % STAGES, r = it / STAGES;
+                    if (!umma::mbar_wait_or_abort(&full[s], r & 1u, WAIT_BUDGET, abort_v)) { ok = false; break; }
+                    umma::fence_after_sync();
+                    const uint32_t sa = umma::smem_u32(smem + s * stage_bytes), sb = sa + a_bytes;
+#pragma unroll
+                    for (int k = 0; k < TILE_K / 16; ++k)
+                        umma::mma_bf16(d, umma::make_desc_sw128(sa + 32u * k), umma::make_desc_sw128(sb + 32u * k),
+                                       idesc, (c > 0 || k > 0) ? 1u : 0u);
+                    umma::commit(&empty[s]);
+                }
+                if (!ok) break;
+                umma::commit(&acc_full[a]);
+            }
+            if (!ok) { atomicOr(G.err, 1u); *abort_v = 1; }
+            // the last MMAs complete before TMEM is freed
+            if (it > 0) umma::mbar_wait(&empty[(it - 1) % STAGES], ((it - 1) / STAGES) & 1u, WAIT_BUDGET);
+        }
+    } else {
+        float* red = red_all + warp * (32 * RED_STRIDE + 32 * 3);
+        uint32_t j = 0;
+        for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++j) {
+            const uint32_t a = j & 1u, u = j >> 1;
+            if (!umma::mbar_wait_or_abort(&acc_full[a], u & 1u, WAIT_BUDGET, abort_v)) {
+                if (lane == 0) atomicOr(G.err, 1u);
+                *abort_v = 1;
+                break;
+            }
+            umma::fence_after_sync();
+            const int row = tile * TILE_M + 32 * warp + lane;
+            epilogue<EPI>(G, tmem + a * 256u + ((uint32_t)(32 * warp) << 16), row, red, lane);
+            umma::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) umma::mbar_arrive(&acc_empty[a]);
+        }
     }
     __syncthreads();
-    if (warp == 0) umma::tmem_dealloc(tmem, 256);
+    if (warp == 5) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(tmem, TMEM_COLS);
+    }
 }
 
-// ---- host launch helper ----
-template <int EPI>
-int launch_gemm(const GemmArgs& g, int grid_x, int splits, cudaStream_t st)
+// ---- host side: tensor maps and launches ----
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+
+bool encoder()
 {
-    if (g.M % TILE_M || g.N % 32 || g.N > 256 || g.N < 32 || g.K % TILE_K || splits < 1)
+    std::call_once(g_encode_once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        cudaGetLastError();
+    });
+    return g_encode != nullptr;
+}
+
+// rows x K BF16 matrix with row stride ld (elements), boxes of 64 x box_rows,
+// 128-byte swizzle.
+bool make_map(CUtensorMap* m, const bf16* base, int64_t rows, int64_t K, int64_t ld, int box_rows)
+{
+    if (!encoder() || ((uintptr_t)base & 15) || (ld * 2) % 16 || K % TILE_K) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+    const cuuint32_t box[2] = {(cuuint32_t)TILE_K, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// A [M][K] (row stride lda), B [N][K] (row stride ldb).
+template <int EPI>
+int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int grid_x,
+                int splits, cudaStream_t st)
+{
+    if (g.M % TILE_M || g.M <= 0 || g.N % 32 || g.N > 256 || g.N < 32 || g.K % TILE_K || g.K <= 0 ||
+        splits < 1 || g.k_split % TILE_K || g.k_split <= 0 || (int64_t)(splits - 1) * g.k_split >= g.K ||
+        (int64_t)splits * g.k_split < g.K || grid_x < 1)
         return CL_ERR_ARG;
-    // The request is padded to 100 KB so that at most two CTAs share an SM:
-    // each holds 256 of the SM's 512 TMEM columns.
-    const size_t need = (size_t)TILE_M * TILE_K * 2 + (size_t)g.N * TILE_K * 2;
-    const size_t smem = need > GEMM_SMEM_BYTES ? need : GEMM_SMEM_BYTES;
+    CUtensorMap ta, tb;
+    if (!make_map(&ta, A, g.M, g.K, lda, TILE_M) || !make_map(&tb, B, g.N, g.K, ldb, g.N)) return CL_ERR_ARG;
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(gemm_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)GEMM_SMEM_BYTES);
+                             (int)gemm_smem_bytes(256));
         attr_set = true;
     }
-    dim3 grid((unsigned)grid_x, (unsigned)splits);
-    gemm_kernel<EPI><<<grid, GEMM_THREADS, smem, st>>>(g);
+    const int tiles = g.M / TILE_M;
+    dim3 grid((unsigned)(grid_x < tiles ? grid_x : tiles), (unsigned)splits);
+    // at least 116 KB so that one CTA holds an SM: each allocates all 512 TMEM columns
+    const size_t smem = gemm_smem_bytes(g.N) > 116 * 1024 ? gemm_smem_bytes(g.N) : 116 * 1024;
+    gemm_kernel<EPI><<<grid, GEMM_THREADS, smem, st>>>(ta, tb, g);
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
 }
 
@@ -240,38 +411,33 @@ __global__ void gather_batch(const float* __restrict__ X, const float* __restric
     for (int j = threadIdx.x; j < D_OUT; j += blockDim.x) Tb[(int64_t)b * D_OUT + j] = T[i * D_OUT + j];
 }
 
-// Layer 1 (K = 3) on the CUDA cores: z = x W1^T + b1, h = silu(z).
-__global__ void layer1_fwd(const float* __restrict__ X, const float* __restrict__ W1, const float* __restrict__ b1,
-                           int B, bf16* H, bf16* Ht, bf16* Z)
+// Layer 1 (K = 3) on the CUDA cores: h = silu(x W1^T + b1) for 64 rows per
+// block, one thread per feature; H rows and (optionally) H^T rows go out
+// coalesced through a shared tile.
+constexpr int L1_ROWS = 64;
+__global__ void __launch_bounds__(256) layer1_fwd(const float* __restrict__ X, const float* __restrict__ W1,
+                                                  const float* __restrict__ b1, int B, bf16* H, bf16* Ht)
 {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)B * D_H) return;
-    const int b = (int)(idx / D_H), j = (int)(idx % D_H);
-    const float* x = X + (int64_t)b * D_IN;
-    const float z = b1[j] + x[0] * W1[j * D_IN] + x[1] * W1[j * D_IN + 1] + x[2] * W1[j * D_IN + 2];
-    const bf16 h = __float2bfloat16_rn(silu(z));
-    H[idx] = h;
-    if (Z) Z[idx] = __float2bfloat16_rn(z);
-    if (Ht) Ht[(int64_t)j * B + b] = h;
-}
-
-// Loss 1/(B*192) sum (o - t)^2 and its gradient dO (BF16, row and transposed).
-__global__ void loss_grad(const float* __restrict__ O, const float* __restrict__ Tb, int B, float scale,
-                          bf16* dO, bf16* dOt, float* loss_acc)
-{
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    float sq = 0.0f;
-    if (idx < (int64_t)B * D_OUT) {
-        const int b = (int)(idx / D_OUT), j = (int)(idx % D_OUT);
-        const float d = O[idx] - Tb[idx];
-        sq = d * d;
-        const bf16 g = __float2bfloat16_rn(2.0f * d * scale);
-        dO[idx] = g;
-        dOt[(int64_t)j * B + b] = g;
+    __shared__ float xs[L1_ROWS * 3];
+    __shared__ __align__(16) bf16 hs[D_H][L1_ROWS + 8];
+    const int b0 = blockIdx.x * L1_ROWS;
+    for (int i = threadIdx.x; i < L1_ROWS * 3; i += blockDim.x) xs[i] = X[(int64_t)b0 * 3 + i];
+    __syncthreads();
+    const int j = threadIdx.x;
+    const float w0 = W1[j * 3], w1 = W1[j * 3 + 1], w2 = W1[j * 3 + 2], bj = b1[j];
+    for (int r = 0; r < L1_ROWS; ++r) {
+        // same operations, same order as the layer-1 recompute in the backward epilogue
+        const float z = bj + xs[r * 3] * w0 + xs[r * 3 + 1] * w1 + xs[r * 3 + 2] * w2;
+        const bf16 h = __float2bfloat16_rn(silu(z));
+        H[(int64_t)(b0 + r) * D_H + j] = h;
+        hs[j][r] = h;
     }
-    if (loss_acc) {
-        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-        if ((threadIdx.x & 31) == 0 && sq != 0.0f) atomicAdd(loss_acc, sq * scale);
+    if (!Ht) return;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < D_H * (L1_ROWS / 2); idx += blockDim.x) {
+        const int jj = idx / (L1_ROWS / 2), q = idx % (L1_ROWS / 2);
+        *reinterpret_cast<__nv_bfloat162*>(Ht + (int64_t)jj * B + b0 + 2 * q) =
+            *reinterpret_cast<const __nv_bfloat162*>(&hs[jj][2 * q]);
     }
 }
 
@@ -284,36 +450,6 @@ __global__ void reduce_wgrad(const float* __restrict__ P, int S, int IN, int OUT
     float acc = 0.0f;
     for (int s = 0; s < S; ++s) acc += P[((int64_t)s * IN + i) * OUT + o];
     gWt[(int64_t)o * IN + i] = acc;
-}
-
-// Row sums of a [R][B] BF16 matrix (bias gradients from transposed gradients);
-// with X, also the layer-1 weight gradients g1[r][k] = sum_b G[r][b] X[b][k].
-__global__ void row_sums(const bf16* __restrict__ G, int B, float* gb, const float* __restrict__ X, float* g1)
-{
-    const int r = blockIdx.x;
-    float s = 0.0f, w0 = 0.0f, w1 = 0.0f, w2 = 0.0f;
-    for (int b = threadIdx.x; b < B; b += blockDim.x) {
-        const float g = __bfloat162float(G[(int64_t)r * B + b]);
-        s += g;
-        if (X) { w0 += g * X[(int64_t)b * 3]; w1 += g * X[(int64_t)b * 3 + 1]; w2 += g * X[(int64_t)b * 3 + 2]; }
-    }
-    __shared__ float red[4][32];
-    for (int o = 16; o > 0; o >>= 1) {
-        s += __shfl_xor_sync(0xffffffffu, s, o);
-        w0 += __shfl_xor_sync(0xffffffffu, w0, o);
-        w1 += __shfl_xor_sync(0xffffffffu, w1, o);
-        w2 += __shfl_xor_sync(0xffffffffu, w2, o);
-    }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { red[0][w] = s; red[1][w] = w0; red[2][w] = w1; red[3][w] = w2; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float a[4] = {0, 0, 0, 0};
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i)
-            for (int q = 0; q < 4; ++q) a[q] += red[q][i];
-        gb[r] = a[0];
-        if (X) { g1[r * 3] = a[1]; g1[r * 3 + 1] = a[2]; g1[r * 3 + 2] = a[3]; }
-    }
 }
 
 // Adam on an FP32 master tensor; optional BF16 copies of a [OUT][IN] matrix
@@ -366,6 +502,7 @@ struct cl_mlp {
     int device = 0;
     int max_batch = 0;
     int num_sms = 0;
+    int max_ctas = 0;               // cap on the GEMM grid (0: one CTA per SM)
     cudaStream_t stream = nullptr;
     char err[256] = {0};
     // FP32 master parameters, gradients, Adam moments
@@ -375,10 +512,9 @@ struct cl_mlp {
     bf16 *w2t = nullptr, *w2 = nullptr, *w3t = nullptr, *w3 = nullptr, *w4t = nullptr, *w4 = nullptr;
     // activations and gradients (max_batch rows)
     float *xb = nullptr, *tb = nullptr, *o = nullptr;
-    bf16 *h1 = nullptr, *h1t = nullptr, *z1 = nullptr, *h2 = nullptr, *h2t = nullptr, *z2 = nullptr;
+    bf16 *h1 = nullptr, *h1t = nullptr, *h2 = nullptr, *h2t = nullptr, *z2 = nullptr;
     bf16 *h3 = nullptr, *h3t = nullptr, *z3 = nullptr;
     bf16 *dO = nullptr, *dOt = nullptr, *dz3 = nullptr, *dz3t = nullptr, *dz2 = nullptr, *dz2t = nullptr;
-    bf16 *dz1 = nullptr, *dz1t = nullptr;
     float* part = nullptr;          // split-K partials
     float* loss = nullptr;          // device accumulator
     unsigned int* derr = nullptr;
@@ -417,84 +553,82 @@ void refresh_bf16(cl_mlp* m, cudaStream_t st)
     to_bf16_pair<<<(D_OUT * D_H + 255) / 256, 256, 0, st>>>(m->p + OFF_W4, D_OUT, D_H, m->w4t, m->w4);
 }
 
-// Forward pass over B rows of m->xb (B % 128 == 0): activations and O.
-int forward(cl_mlp* m, int B, bool keep_t, cudaStream_t st)
+int grid_for(const cl_mlp* m, int B)
 {
     const int tiles = B / TILE_M;
-    const int grid = tiles < 2 * m->num_sms ? tiles : 2 * m->num_sms;
-    layer1_fwd<<<(unsigned)(((int64_t)B * D_H + 255) / 256), 256, 0, st>>>(
-        m->xb, m->p + OFF_W1, m->p + OFF_B1, B, m->h1, keep_t ? m->h1t : nullptr, m->z1);
-    GemmArgs g;
-    memset(&g, 0, sizeof g);
-    g.err = m->derr;
-    g.M = B; g.K = D_H; g.k_split = D_H;
-    // layer 2
-    g.A = m->h1; g.lda = D_H; g.B = m->w2t; g.ldb = D_H; g.N = D_H;
-    g.bias = m->p + OFF_B2; g.out_h = m->h2; g.ldh = D_H; g.out_ht = keep_t ? m->h2t : nullptr; g.ldht = B;
-    g.out_z = m->z2;
-    int rc = launch_gemm<EPI_BIAS_SILU>(g, grid, 1, st);
-    if (rc) return rc;
-    // layer 3
-    g.A = m->h2; g.B = m->w3t; g.bias = m->p + OFF_B3; g.out_h = m->h3;
-    g.out_ht = keep_t ? m->h3t : nullptr; g.out_z = m->z3;
-    if ((rc = launch_gemm<EPI_BIAS_SILU>(g, grid, 1, st))) return rc;
-    // layer 4 (linear)
-    GemmArgs q;
-    memset(&q, 0, sizeof q);
-    q.err = m->derr;
-    q.M = B; q.K = D_H; q.k_split = D_H; q.N = D_OUT;
-    q.A = m->h3; q.lda = D_H; q.B = m->w4t; q.ldb = D_H;
-    q.bias = m->p + OFF_B4; q.out_f = m->o; q.ldf = D_OUT;
-    return launch_gemm<EPI_BIAS_F32>(q, grid, 1, st);
+    const int cap = m->max_ctas > 0 && m->max_ctas < m->num_sms ? m->max_ctas : m->num_sms;
+    return tiles < cap ? tiles : cap;
 }
 
-// Backward pass for the batch in m->xb / m->tb (forward already run with
-// keep_t): gradients into m->g.
-int backward(cl_mlp* m, int B, cudaStream_t st)
+GemmArgs gemm_args(cl_mlp* m)
 {
-    const int tiles = B / TILE_M;
-    const int grid = tiles < 2 * m->num_sms ? tiles : 2 * m->num_sms;
-    const float scale = 1.0f / ((float)B * (float)D_OUT);
-    loss_grad<<<(unsigned)(((int64_t)B * D_OUT + 255) / 256), 256, 0, st>>>(m->o, m->tb, B, scale, m->dO,
-                                                                             m->dOt, m->loss);
-    // backward data: dZ3 = (dO W4) * silu'(Z3), dZ2 = (dZ3 W3) * silu'(Z2), dZ1 = (dZ2 W2) * silu'(Z1)
     GemmArgs g;
     memset(&g, 0, sizeof g);
     g.err = m->derr;
-    g.M = B; g.N = D_H;
-    g.A = m->dO; g.lda = D_OUT; g.K = D_OUT; g.k_split = D_OUT;
-    g.B = m->w4; g.ldb = D_OUT;
-    g.out_h = m->dz3; g.ldh = D_H; g.out_ht = m->dz3t; g.ldht = B; g.zprev = m->z3;
-    int rc = launch_gemm<EPI_DSILU>(g, grid, 1, st);
+    return g;
+}
+
+// Forward pass over B rows of m->xb (B % 128 == 0).  Training (with_loss):
+// keeps Z, H^T for the backward pass and ends in the loss epilogue, which
+// writes dO, dO^T, the b4 gradient and the loss.  Inference: O into m->o.
+int forward(cl_mlp* m, int B, bool with_loss, cudaStream_t st)
+{
+    const int grid = grid_for(m, B);
+    if (with_loss) cudaMemsetAsync(m->g, 0, N_PARAMS * sizeof(float), st);
+    layer1_fwd<<<(unsigned)(B / L1_ROWS), 256, 0, st>>>(m->xb, m->p + OFF_W1, m->p + OFF_B1, B, m->h1,
+                                                         with_loss ? m->h1t : nullptr);
+    GemmArgs g = gemm_args(m);
+    g.M = B; g.N = D_H; g.K = D_H; g.k_split = D_H;
+    g.bias = m->p + OFF_B2; g.out_h = m->h2; g.ldh = D_H;
+    g.out_ht = with_loss ? m->h2t : nullptr; g.ldht = B; g.out_z = with_loss ? m->z2 : nullptr;
+    int rc = launch_gemm<EPI_BIAS_SILU>(g, m->h1, D_H, m->w2t, D_H, grid, 1, st);
     if (rc) return rc;
-    g.A = m->dz3; g.lda = D_H; g.K = D_H; g.k_split = D_H;
-    g.B = m->w3; g.ldb = D_H;
-    g.out_h = m->dz2; g.out_ht = m->dz2t; g.zprev = m->z2;
-    if ((rc = launch_gemm<EPI_DSILU>(g, grid, 1, st))) return rc;
-    g.A = m->dz2; g.B = m->w2;
-    g.out_h = m->dz1; g.out_ht = m->dz1t; g.zprev = m->z1;
-    if ((rc = launch_gemm<EPI_DSILU>(g, grid, 1, st))) return rc;
+    g.bias = m->p + OFF_B3; g.out_h = m->h3;
+    g.out_ht = with_loss ? m->h3t : nullptr; g.out_z = with_loss ? m->z3 : nullptr;
+    if ((rc = launch_gemm<EPI_BIAS_SILU>(g, m->h2, D_H, m->w3t, D_H, grid, 1, st))) return rc;
+    GemmArgs q = gemm_args(m);
+    q.M = B; q.N = D_OUT; q.K = D_H; q.k_split = D_H; q.bias = m->p + OFF_B4;
+    if (!with_loss) {
+        q.out_f = m->o; q.ldf = D_OUT;
+        return launch_gemm<EPI_BIAS_F32>(q, m->h3, D_H, m->w4t, D_H, grid, 1, st);
+    }
+    q.target = m->tb; q.scale = 1.0f / ((float)B * (float)D_OUT); q.loss = m->loss;
+    q.out_h = m->dO; q.ldh = D_OUT; q.out_ht = m->dOt; q.ldht = B; q.colsum = m->g + OFF_B4;
+    return launch_gemm<EPI_LOSS>(q, m->h3, D_H, m->w4t, D_H, grid, 1, st);
+}
+
+// Backward pass after forward(with_loss), which zeroed m->g: bias and layer-1
+// gradients accumulate in the epilogues, weight gradients come from the
+// split-K GEMMs.
+int backward(cl_mlp* m, int B, cudaStream_t st)
+{
+    const int grid = grid_for(m, B);
+    // backward data: dZ3 = (dO W4) * silu'(Z3), dZ2 = (dZ3 W3) * silu'(Z2), dZ1 = (dZ2 W2) * silu'(Z1)
+    GemmArgs g = gemm_args(m);
+    g.M = B; g.N = D_H; g.K = D_OUT; g.k_split = D_OUT;
+    g.out_h = m->dz3; g.ldh = D_H; g.out_ht = m->dz3t; g.ldht = B; g.zprev = m->z3; g.colsum = m->g + OFF_B3;
+    int rc = launch_gemm<EPI_DSILU>(g, m->dO, D_OUT, m->w4, D_OUT, grid, 1, st);
+    if (rc) return rc;
+    g.K = D_H; g.k_split = D_H;
+    g.out_h = m->dz2; g.out_ht = m->dz2t; g.zprev = m->z2; g.colsum = m->g + OFF_B2;
+    if ((rc = launch_gemm<EPI_DSILU>(g, m->dz3, D_H, m->w3, D_H, grid, 1, st))) return rc;
+    GemmArgs l1 = gemm_args(m);
+    l1.M = B; l1.N = D_H; l1.K = D_H; l1.k_split = D_H;
+    l1.bias = m->p + OFF_B1; l1.x = m->xb; l1.w1 = m->p + OFF_W1;
+    l1.colsum = m->g + OFF_B1; l1.gw1 = m->g + OFF_W1;
+    if ((rc = launch_gemm<EPI_DSILU_L1>(l1, m->dz2, D_H, m->w2, D_H, grid, 1, st))) return rc;
     // weight gradients dW = H^T dZ (split-K over the batch) -> grad W^T
     const int splits = (B + WGRAD_SPLIT_K - 1) / WGRAD_SPLIT_K;
-    struct WG { const bf16* ht; const bf16* dzt; int OUT; int64_t off_w; int64_t off_b; };
-    const WG wg[3] = {{m->h3t, m->dOt, D_OUT, OFF_W4, OFF_B4},
-                      {m->h2t, m->dz3t, D_H, OFF_W3, OFF_B3},
-                      {m->h1t, m->dz2t, D_H, OFF_W2, OFF_B2}};
+    struct WG { const bf16* ht; const bf16* dzt; int OUT; int64_t off_w; };
+    const WG wg[3] = {{m->h3t, m->dOt, D_OUT, OFF_W4}, {m->h2t, m->dz3t, D_H, OFF_W3}, {m->h1t, m->dz2t, D_H, OFF_W2}};
     for (int l = 0; l < 3; ++l) {
-        GemmArgs w;
-        memset(&w, 0, sizeof w);
-        w.err = m->derr;
-        w.A = wg[l].ht; w.lda = B; w.M = D_H;
-        w.B = wg[l].dzt; w.ldb = B; w.N = wg[l].OUT;
-        w.K = B; w.k_split = WGRAD_SPLIT_K;
+        GemmArgs w = gemm_args(m);
+        w.M = D_H; w.N = wg[l].OUT; w.K = B; w.k_split = WGRAD_SPLIT_K;
         w.out_f = m->part; w.ldf = wg[l].OUT;
-        if ((rc = launch_gemm<EPI_PARTIAL>(w, D_H / TILE_M, splits, st))) return rc;
+        if ((rc = launch_gemm<EPI_PARTIAL>(w, wg[l].ht, B, wg[l].dzt, B, D_H / TILE_M, splits, st))) return rc;
         reduce_wgrad<<<(D_H * wg[l].OUT + 255) / 256, 256, 0, st>>>(m->part, splits, D_H, wg[l].OUT,
                                                                     m->g + wg[l].off_w);
-        row_sums<<<wg[l].OUT, 256, 0, st>>>(wg[l].dzt, B, m->g + wg[l].off_b, nullptr, nullptr);
     }
-    // layer 1: bias and weight gradients from dZ1^T and X
-    row_sums<<<D_H, 256, 0, st>>>(m->dz1t, B, m->g + OFF_B1, m->xb, m->g + OFF_W1);
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
 }
 
@@ -546,13 +680,12 @@ int cl_mlp_create(cl_mlp** out, int device, int max_batch)
               dalloc(m, &m->w3t, (size_t)D_H * D_H) && dalloc(m, &m->w3, (size_t)D_H * D_H) &&
               dalloc(m, &m->w4t, (size_t)D_OUT * D_H) && dalloc(m, &m->w4, (size_t)D_OUT * D_H) &&
               dalloc(m, &m->xb, B * D_IN) && dalloc(m, &m->tb, B * D_OUT) && dalloc(m, &m->o, B * D_OUT) &&
-              dalloc(m, &m->h1, B * D_H) && dalloc(m, &m->h1t, B * D_H) && dalloc(m, &m->z1, B * D_H) &&
+              dalloc(m, &m->h1, B * D_H) && dalloc(m, &m->h1t, B * D_H) &&
               dalloc(m, &m->h2, B * D_H) && dalloc(m, &m->h2t, B * D_H) && dalloc(m, &m->z2, B * D_H) &&
               dalloc(m, &m->h3, B * D_H) && dalloc(m, &m->h3t, B * D_H) && dalloc(m, &m->z3, B * D_H) &&
               dalloc(m, &m->dO, B * D_OUT) && dalloc(m, &m->dOt, B * D_OUT) &&
               dalloc(m, &m->dz3, B * D_H) && dalloc(m, &m->dz3t, B * D_H) &&
               dalloc(m, &m->dz2, B * D_H) && dalloc(m, &m->dz2t, B * D_H) &&
-              dalloc(m, &m->dz1, B * D_H) && dalloc(m, &m->dz1t, B * D_H) &&
               dalloc(m, &m->part, (size_t)splits * D_H * D_H) && dalloc(m, &m->loss, 1) &&
               dalloc(m, &m->derr, 1);
     if (!ok) {
@@ -582,6 +715,15 @@ void cl_mlp_destroy(cl_mlp* m)
 }
 
 const char* cl_mlp_last_error(const cl_mlp* m) { return m ? m->err : ""; }
+
+// Cap the number of CTAs of the row-tiled GEMMs (0 = one per SM); with few
+// CTAs each one walks many tiles (tests of the persistent pipeline).
+int cl_mlp_set_max_ctas(cl_mlp* m, int n)
+{
+    if (!m || n < 0) return CL_ERR_ARG;
+    m->max_ctas = n;
+    return CL_OK;
+}
 
 // Parameters in the FP32 block layout above (host buffers of cl_mlp_param_count()).
 // Setting parameters resets the Adam state.
@@ -697,20 +839,19 @@ extern "C" {
 int cl_umma_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, int grid_x,
                       int splits, unsigned int* d_err, void* stream)
 {
-    if (!A || !B || !C || !d_err || M <= 0 || N <= 0 || K <= 0 || grid_x <= 0) return CL_ERR_ARG;
+    if (!A || !B || !C || !d_err || M <= 0 || N <= 0 || K <= 0 || grid_x <= 0 || splits < 1) return CL_ERR_ARG;
     GemmArgs g;
     memset(&g, 0, sizeof g);
-    g.A = (const bf16*)A; g.lda = K;
-    g.B = (const bf16*)B; g.ldb = K;
     g.M = M; g.N = N; g.K = K;
     g.out_f = C; g.ldf = N;
     g.err = d_err;
     if (splits > 1) {
         g.k_split = ((K / splits + TILE_K - 1) / TILE_K) * TILE_K;
-        return launch_gemm<EPI_PARTIAL>(g, grid_x, splits, (cudaStream_t)stream);
+        return launch_gemm<EPI_PARTIAL>(g, (const bf16*)A, K, (const bf16*)B, K, grid_x, splits,
+                                        (cudaStream_t)stream);
     }
     g.k_split = K;
-    return launch_gemm<EPI_F32>(g, grid_x, 1, (cudaStream_t)stream);
+    return launch_gemm<EPI_F32>(g, (const bf16*)A, K, (const bf16*)B, K, grid_x, 1, (cudaStream_t)stream);
 }
 
 }  // extern "C"

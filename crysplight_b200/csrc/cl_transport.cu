@@ -66,6 +66,8 @@ struct KArgs {
     uint32_t* counts;     // point: cells*bins_total
     uint32_t* keys;       // point: cells; segments: cells*n_seg
     uint32_t* maps;       // segments: cells*n_seg
+    unsigned long long* tsum;   // segments with moments (MODE 2): cells*n_seg
+    unsigned long long* tsum2;
     unsigned long long* counters;  // 9 x int64, cl_counters order
     uint8_t* r_status; int16_t* r_idx; float* r_t; int32_t* r_bounces;
     unsigned long long* queue;
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
                     pool_lo = (int64_t)base;
                     pool_hi = pool_lo + A.warp_chunk;
                     if (pool_hi > A.n) pool_hi = A.n;
-                    if (MODE == 1) {
+                    if (MODE != 0) {
                         int64_t s0 = 0;
                         if (lane == 0) s0 = find_source(A.src_off, A.n_src, pool_src, pool_lo);
                         pool_src = __shfl_sync(FULL, s0, 0);
@@ -490,6 +492,12 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
                 const unsigned g = __match_any_sync(dmask, slot);
                 if (lane == __ffs(g) - 1) atomicAdd(A.maps + slot, (uint32_t)__popc(g));
                 atomicMin(A.keys + slot, key);
+                if (MODE == 2) {
+                    // fixed-point time moments (exact integer sums, order-independent)
+                    const float tc = fminf(fmaxf(t, 0.0f), CL_MOMENT_T_MAX_NS);
+                    atomicAdd(A.tsum + slot, __float2ull_rn(tc * CL_MOMENT_T_SCALE));
+                    atomicAdd(A.tsum2 + slot, __float2ull_rn((tc * tc) * CL_MOMENT_T2_SCALE));
+                }
             }
         }
 
@@ -762,6 +770,7 @@ int cl_create(cl_handle** out, int device)
     set_kernel_attrs<0, true, false>(h->max_smem_optin);
     set_kernel_attrs<1, false, false>(h->max_smem_optin);
     set_kernel_attrs<1, true, false>(h->max_smem_optin);
+    set_kernel_attrs<2, false, false>(h->max_smem_optin);
     cudaGetLastError();
     if (ensure(h, h->scratch, 64) != CL_OK) {
         snprintf(g_create_err, sizeof g_create_err, "cl_create: %s", h->err);
@@ -938,7 +947,8 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
                             const float* sz, const float* sT, const int64_t* off, const int32_t* segid,
                             int64_t n_src, int64_t n_seg, int64_t n, uint64_t pid0,
                             uint32_t* maps, uint32_t* keys, int32_t* npe,
-                            unsigned long long* counters, const cl_records* rec, cudaStream_t st)
+                            unsigned long long* counters, const cl_records* rec, cudaStream_t st,
+                            unsigned long long* tsum = nullptr, unsigned long long* tsum2 = nullptr)
 {
     const int cells = P.nx * P.ny;
     const int64_t total = (int64_t)cells * n_seg;
@@ -946,6 +956,11 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
     init_kernel<<<(unsigned)std::min<int64_t>((total + 255) / 256 + 1, 8192), 256, 0, st>>>(
         maps, total, keys, total, counters, s.queue, s.steps, s.done, s.err);
     CK(h, cudaGetLastError(), "init kernel launch");
+    const bool moments = tsum && tsum2;
+    if (moments) {
+        CK(h, cudaMemsetAsync(tsum, 0, (size_t)total * sizeof(unsigned long long), st), "zero moments");
+        CK(h, cudaMemsetAsync(tsum2, 0, (size_t)total * sizeof(unsigned long long), st), "zero moments");
+    }
     if (n > 0) {
         KArgs a;
         memset(&a, 0, sizeof a);
@@ -958,7 +973,9 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
         if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
         a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
         const size_t smem = LOGTAB_BYTES + (size_t)RING_LEN * RING_STRIDE * sizeof(float);
-        const int rc = want_rec ? launch_transport<1, true, false>(h, a, smem, st)
+        a.tsum = tsum; a.tsum2 = tsum2;
+        const int rc = moments ? launch_transport<2, false, false>(h, a, smem, st)
+                     : want_rec ? launch_transport<1, true, false>(h, a, smem, st)
                                 : launch_transport<1, false, false>(h, a, smem, st);
         if (rc != CL_OK) return rc;
     }
@@ -1203,6 +1220,36 @@ int cl_run_segments_device(cl_handle* h, const cl_box* box, const cl_optical_par
     return enqueue_segments(h, P, d_sx, d_sy, d_sz, d_st, d_src_offsets, d_src_segment, n_src, n_segments,
                             n, pid_offset, d_maps, (uint32_t*)d_tmin, d_npe,
                             (unsigned long long*)d_counters, d_records, st);
+}
+
+int cl_run_segments_moments_device(cl_handle* h, const cl_box* box, const cl_optical_params* op,
+                                   const cl_readout* ro, const cl_time_binning* tb,
+                                   const float* d_sx, const float* d_sy, const float* d_sz,
+                                   const float* d_st, const int64_t* d_src_offsets,
+                                   const int32_t* d_src_segment, int64_t n_src, int64_t n_segments,
+                                   int64_t n_photons, uint64_t seed, uint64_t pid_offset,
+                                   float tau_ns, int32_t max_bounces,
+                                   uint32_t* d_maps, float* d_tmin, int32_t* d_npe,
+                                   cl_counters* d_counters, uint64_t* d_tsum, uint64_t* d_tsum2,
+                                   void* stream)
+{
+    if (!h) return CL_ERR_STATE;
+    h->err[0] = 0;
+    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    if (rc != CL_OK) return rc;
+    if (n_src < 1 || n_segments < 1) return set_err(h, CL_ERR_ARG, "need n_src >= 1 and n_segments >= 1");
+    if (!d_sx || !d_sy || !d_sz || !d_src_offsets || !d_src_segment)
+        return set_err(h, CL_ERR_ARG, "null source array");
+    if (!d_maps || !d_tmin || !d_npe || !d_counters || !d_tsum || !d_tsum2)
+        return set_err(h, CL_ERR_ARG, "null output buffer");
+    if (n_photons < 0) return set_err(h, CL_ERR_ARG, "negative photon total");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    const Physics P = make_physics(box, op, ro, tb, tau_ns, max_bounces, seed);
+    return enqueue_segments(h, P, d_sx, d_sy, d_sz, d_st, d_src_offsets, d_src_segment, n_src, n_segments,
+                            n_photons, pid_offset, d_maps, (uint32_t*)d_tmin, d_npe,
+                            (unsigned long long*)d_counters, nullptr, st,
+                            (unsigned long long*)d_tsum, (unsigned long long*)d_tsum2);
 }
 
 int cl_sync(cl_handle* h, void* stream)

@@ -3,7 +3,14 @@
 // accumulator in tensor memory (TMEM), TMEM allocation and loads, and bounded
 // mbarrier waits.
 //
-// Operand layout in shared memory: the canonical K-major layout without
+// Operand layouts in shared memory.  (1) The canonical K-major layout without
+// swizzle (make_desc), staged by ordinary stores.  (2) The K-major layout with
+// the 128-byte swizzle (make_desc_sw128), written by TMA: a tile of R rows x
+// 64 BF16 is R rows of 128 bytes, 8-row groups 1024 bytes apart (SBO), the
+// 16-byte pieces of row r XOR-permuted by (r & 7); a K step of 16 elements
+// advances the start address by 32 bytes inside the swizzle atom.
+//
+// Layout (1) in detail: the canonical K-major layout without
 // swizzle.  A core matrix is 8 rows x 16 bytes (8 BF16 along K), its rows
 // contiguous (128 bytes).  For a tile of R rows x KC K-elements, core matrix
 // (row group g = r/8, K chunk c = k/8) sits at byte ((c * R/8) + g) * 128: row
@@ -41,6 +48,19 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo_bytes
     d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
     d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Descriptor of a 128-byte-swizzled K-major tile (1024-byte aligned base):
+// LBO unused (1), SBO = 1024 bytes, layout type 2 (SWIZZLE_128B) in bits 61-63.
+__device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
     return d;
 }
 
@@ -91,6 +111,51 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t phase, uint32
         if (ok) return true;
     }
     return false;
+}
+
+// Same, but also gives up as soon as *abort is set by another thread.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* mbar, uint32_t phase, uint32_t budget,
+                                                   volatile int* abort)
+{
+    const uint32_t a = smem_u32(mbar);
+    for (uint32_t i = 0; i < budget; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok) : "r"(a), "r"(phase) : "memory");
+        if (ok) return true;
+        if ((i & 63u) == 63u && *abort) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(mbar)) : "memory");
+}
+
+// Arrive and add `bytes` to the transaction count the current phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_u32(mbar)), "r"(bytes) : "memory");
+}
+
+// 2-D tiled TMA load (no multicast) of the box at element coordinates
+// (x = inner, y = row) into shared memory; completion counted on `mbar`.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int32_t x, int32_t y, uint64_t* mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        :: "r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(mbar))
+        : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const void* tmap)
+{
+    asm volatile("prefetch.tensormap [%0];" :: "l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
 }
 
 // Generic-proxy shared-memory writes -> visible to the tensor core (async proxy).

@@ -10,12 +10,13 @@ data is generated by the CUDA Monte Carlo itself (``scan_dataset``).
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 from typing import Optional
 
 import numpy as np
 
 from . import _lib
+from .params import Box, Counters, Readout, TimeBinning
 
 D_IN, D_H, D_OUT = 3, 256, 192
 N_CELLS = 64
@@ -32,6 +33,8 @@ def _declare(lib):
     lib.cl_mlp_destroy.restype = None
     lib.cl_mlp_last_error.argtypes = [P]
     lib.cl_mlp_last_error.restype = C.c_char_p
+    lib.cl_mlp_set_max_ctas.argtypes = [P, C.c_int]
+    lib.cl_mlp_set_max_ctas.restype = C.c_int
     lib.cl_mlp_set_params.argtypes = [P, P]
     lib.cl_mlp_get_params.argtypes = [P, P]
     lib.cl_mlp_set_data.argtypes = [P, P, P, C.c_int64]
@@ -89,6 +92,9 @@ class MLP:
         if rc != 0:
             raise _lib.CudaTransportError(rc, self.lib.cl_mlp_last_error(self.h).decode())
 
+    def set_max_ctas(self, n: int):
+        self._check(self.lib.cl_mlp_set_max_ctas(self.h, int(n)))
+
     def set_params(self, p: np.ndarray):
         p = np.ascontiguousarray(p, np.float32)
         assert p.size == self.n_params
@@ -126,3 +132,197 @@ class MLP:
         self._check(self.lib.cl_mlp_gradient(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(t.data_ptr()),
                                              x.shape[0], C.c_void_p(g.ctypes.data), C.byref(loss)))
         return float(loss.value), g
+
+
+# ---------------------------------------------------------------------------
+# Training data: a point scan through the CUDA Monte Carlo
+# ---------------------------------------------------------------------------
+def grid_points(box: Box, shape=(48, 48, 24)) -> np.ndarray:
+    """Cell centres of a regular nx x ny x nz grid over the crystal, (P, 3)
+    float32 in mm, x fastest."""
+    nx, ny, nz = shape
+    L = [float(box.L[i]) for i in range(3)]
+    ax = [(np.arange(n, dtype=np.float64) + 0.5) * (L[i] / n) for i, n in enumerate((nx, ny, nz))]
+    z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1).astype(np.float32)
+
+
+@dataclass
+class ScanResult:
+    points: np.ndarray          # (P, 3) float32 mm
+    photons_per_point: int
+    counts: np.ndarray          # (P, cells) int64, cell = i + nx*j
+    tsum: np.ndarray            # (P, cells) uint64 fixed-point sums of t
+    tsum2: np.ndarray           # (P, cells) uint64 fixed-point sums of t^2
+    tmin: np.ndarray            # (P, cells) float32
+    counters: dict = field(default_factory=dict)
+    seconds: float = 0.0
+
+
+def scan_light(engine, box: Box, op, ro, *, points: np.ndarray, photons_per_point: int, seed: int,
+               pid_offset: int = 0, batch_points: int = 4096, max_bounces: int = 100_000,
+               tau_ns: float = 0.0) -> ScanResult:
+    """Transport ``photons_per_point`` photons from each point (emitted at
+    t = 0, no decay-time delay by default, so the times are transit times) and
+    collect per-point SiPM counts and arrival-time moments on the GPU."""
+    import time
+    import torch
+    ro = ro if isinstance(ro, Readout) else Readout(ro)
+    cells = ro.grid.nx * ro.grid.ny
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    P = pts.shape[0]
+    npp = int(photons_per_point)
+    dev = torch.device("cuda", engine.device if hasattr(engine, "device") else 0)
+    counts = np.zeros((P, cells), np.int64)
+    tsum = np.zeros((P, cells), np.uint64)
+    tsum2 = np.zeros((P, cells), np.uint64)
+    tmin = np.zeros((P, cells), np.float32)
+    tot = None
+    tb = TimeBinning(100.0, 80)
+    stream = torch.cuda.Stream(device=dev)
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for b0 in range(0, P, batch_points):
+            nb = min(batch_points, P - b0)
+            src = torch.from_numpy(pts[b0:b0 + nb]).to(dev)
+            sx, sy, sz = (src[:, i].contiguous() for i in range(3))
+            off = torch.arange(nb + 1, dtype=torch.int64, device=dev) * npp
+            segid = torch.arange(nb, dtype=torch.int32, device=dev)
+            maps = torch.empty(nb * cells, dtype=torch.int32, device=dev)
+            tm = torch.empty(nb * cells, dtype=torch.float32, device=dev)
+            npe = torch.empty(nb, dtype=torch.int32, device=dev)
+            ctr = torch.zeros(9, dtype=torch.int64, device=dev)
+            s1 = torch.empty(nb * cells, dtype=torch.int64, device=dev)
+            s2 = torch.empty(nb * cells, dtype=torch.int64, device=dev)
+            engine.run_segments_moments_device(
+                box, op, ro, tb, sx=sx.data_ptr(), sy=sy.data_ptr(), sz=sz.data_ptr(), st=None,
+                src_offsets=off.data_ptr(), src_segment=segid.data_ptr(), n_src=nb, n_segments=nb,
+                n_photons=nb * npp, seed=seed, pid_offset=pid_offset + b0 * npp, tau_ns=tau_ns,
+                max_bounces=max_bounces, maps=maps.data_ptr(), tmin=tm.data_ptr(), npe=npe.data_ptr(),
+                counters=ctr.data_ptr(), tsum=s1.data_ptr(), tsum2=s2.data_ptr(),
+                stream=stream.cuda_stream)
+            engine.sync(stream.cuda_stream)
+            counts[b0:b0 + nb] = maps.view(nb, cells).cpu().numpy().astype(np.uint32)
+            tsum[b0:b0 + nb] = s1.view(nb, cells).cpu().numpy().view(np.uint64)
+            tsum2[b0:b0 + nb] = s2.view(nb, cells).cpu().numpy().view(np.uint64)
+            tmin[b0:b0 + nb] = tm.view(nb, cells).cpu().numpy()
+            c = ctr.cpu().numpy()
+            tot = c if tot is None else tot + c
+    from .params import COUNTER_NAMES
+    return ScanResult(pts, npp, counts, tsum, tsum2, tmin,
+                      {n: int(v) for n, v in zip(COUNTER_NAMES, tot)} if tot is not None else {},
+                      time.perf_counter() - t0)
+
+
+MIN_TIME_COUNTS = 20       # below this a cell's time moments are replaced by column medians
+SIGMA_FLOOR_NS = 1e-3
+
+
+def light_targets(scan: ScanResult) -> np.ndarray:
+    """Network targets (P, 192): log detection probability, mean arrival time
+    (ns) and log of its standard deviation, per SiPM."""
+    n = float(scan.photons_per_point)
+    c = scan.counts.astype(np.float64)
+    logp = np.log((c + 0.5) / (n + 1.0))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        m1 = scan.tsum.astype(np.float64) / _lib.MOMENT_T_SCALE / c
+        m2 = scan.tsum2.astype(np.float64) / _lib.MOMENT_T2_SCALE / c
+        var = np.maximum(m2 - m1 * m1, SIGMA_FLOOR_NS ** 2)
+        logs = 0.5 * np.log(var)
+    ok = c >= MIN_TIME_COUNTS
+    for a in (m1, logs):
+        med = np.array([np.median(a[ok[:, j], j]) if ok[:, j].any() else 0.0 for j in range(a.shape[1])])
+        a[~ok] = np.broadcast_to(med, a.shape)[~ok]
+    return np.concatenate([logp, m1, logs], axis=1).astype(np.float32)
+
+
+def split_holdout(n_points: int, frac: float = 0.1, seed: int = 11):
+    """Deterministic train / held-out split of point indices."""
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(n_points)
+    n_hold = int(round(frac * n_points))
+    return np.sort(perm[n_hold:]), np.sort(perm[:n_hold])
+
+
+# ---------------------------------------------------------------------------
+# Ensemble
+# ---------------------------------------------------------------------------
+@dataclass
+class LightSurrogate:
+    """K networks plus the input scaling and the target standardisation."""
+    box_mm: np.ndarray          # (3,)
+    y_mean: np.ndarray          # (192,)
+    y_std: np.ndarray           # (192,)
+    members: list               # K parameter vectors (float32)
+    cells: int = N_CELLS
+    meta: dict = field(default_factory=dict)
+
+    def normalise(self, xyz: np.ndarray) -> np.ndarray:
+        return (2.0 * np.asarray(xyz, np.float32) / self.box_mm.astype(np.float32) - 1.0).astype(np.float32)
+
+    @classmethod
+    def train(cls, box: Box, xyz: np.ndarray, targets: np.ndarray, *, members: int = 5, steps: int = 20000,
+              batch: int = 65536, lr: float = 1e-3, seed: int = 0, device: int = 0,
+              chunk: int = 500, log=None):
+        import time
+        import torch
+        L = np.array([float(box.L[i]) for i in range(3)], np.float64)
+        y_mean = targets.mean(0).astype(np.float64)
+        y_std = np.maximum(targets.std(0), 1e-6).astype(np.float64)
+        obj = cls(L, y_mean.astype(np.float32), y_std.astype(np.float32), [])
+        x = torch.from_numpy(obj.normalise(xyz)).to(f"cuda:{device}")
+        y = torch.from_numpy(((targets - y_mean) / y_std).astype(np.float32)).to(f"cuda:{device}")
+        history = []
+        t0 = time.perf_counter()
+        for k in range(members):
+            net = MLP(device, max_batch=batch, seed=seed * 1000 + k)
+            net.set_data(x, y)
+            hist = []
+            for s0 in range(0, steps, chunk):
+                ns = min(chunk, steps - s0)
+                hist.append(net.train(ns, batch=batch, lr=lr, seed=seed * 1000 + k))
+                if log:
+                    log(f"member {k} step {s0 + ns}: loss {hist[-1]:.5f}")
+            obj.members.append(net.get_params())
+            history.append(hist)
+            net.close()
+        obj.meta = {"steps": steps, "batch": batch, "lr": lr, "seed": seed,
+                    "train_seconds": time.perf_counter() - t0, "loss_history": history}
+        return obj
+
+    def raw_outputs(self, xyz: np.ndarray, device: int = 0):
+        """Standardised outputs of every member: torch tensor (K, n, 192) on the GPU."""
+        import torch
+        x = torch.from_numpy(self.normalise(xyz)).to(f"cuda:{device}")
+        outs = []
+        net = MLP(device, max_batch=65536, seed=0)
+        try:
+            for p in self.members:
+                net.set_params(p)
+                outs.append(net.forward(x))
+        finally:
+            net.close()
+        return torch.stack(outs)
+
+    def predict(self, xyz: np.ndarray, device: int = 0) -> dict:
+        """Ensemble means (numpy): p (n, cells), t_mean, t_sigma (ns), and the
+        count-weighted relative spread of the members' p (n,)."""
+        raw = self.raw_outputs(xyz, device).double().cpu().numpy()
+        y = raw * self.y_std.astype(np.float64) + self.y_mean.astype(np.float64)
+        c = self.cells
+        p = np.exp(y[:, :, :c])
+        pm = p.mean(0)
+        spread = p.std(0).sum(1) / np.maximum(pm.sum(1), 1e-30)
+        return {"p": pm, "t_mean": y[:, :, c:2 * c].mean(0), "t_sigma": np.exp(y[:, :, 2 * c:].mean(0)),
+                "spread": spread, "p_members": p}
+
+    def save(self, path: str):
+        np.savez_compressed(path, box_mm=self.box_mm, y_mean=self.y_mean, y_std=self.y_std,
+                            members=np.stack(self.members), cells=self.cells,
+                            meta=np.array(repr({k: v for k, v in self.meta.items() if k != "loss_history"})))
+
+    @classmethod
+    def load(cls, path: str):
+        z = np.load(path, allow_pickle=False)
+        return cls(z["box_mm"], z["y_mean"], z["y_std"], list(z["members"]), int(z["cells"]),
+                   {"saved": str(z["meta"])})

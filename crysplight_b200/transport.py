@@ -200,6 +200,21 @@ class Engine:
             C.c_void_p(stream) if stream else None)
         self._check(rc)
 
+    def run_segments_moments_device(self, box, op, ro, tb, *, sx, sy, sz, st, src_offsets, src_segment,
+                                    n_src, n_segments, n_photons, seed, pid_offset=0, tau_ns,
+                                    max_bounces=100_000, maps, tmin, npe, counters, tsum, tsum2,
+                                    stream=None) -> None:
+        """run_segments_device plus fixed-point arrival-time sums per (segment, SiPM)."""
+        ro = _as_readout(ro)
+        rc = self.lib.cl_run_segments_moments_device(
+            self.handle, C.byref(box), C.byref(op), C.byref(ro), C.byref(tb),
+            C.c_void_p(sx), C.c_void_p(sy), C.c_void_p(sz), C.c_void_p(st) if st else None,
+            C.c_void_p(src_offsets), C.c_void_p(src_segment), int(n_src), int(n_segments),
+            int(n_photons), int(seed), int(pid_offset), float(np.float32(tau_ns)), int(max_bounces),
+            C.c_void_p(maps), C.c_void_p(tmin), C.c_void_p(npe), C.c_void_p(counters),
+            C.c_void_p(tsum), C.c_void_p(tsum2), C.c_void_p(stream) if stream else None)
+        self._check(rc)
+
     def sync(self, stream=None) -> None:
         self._check(self.lib.cl_sync(self.handle, C.c_void_p(stream) if stream else None))
 

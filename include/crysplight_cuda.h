@@ -233,6 +233,31 @@ int cl_run_segments_device(cl_handle* h,
                            cl_counters* d_counters, const cl_records* d_records,
                            void* stream);
 
+/* cl_run_segments_device plus per-(segment, SiPM) arrival-time moments, the
+ * training targets of the light-response surrogate (no counterpart in the
+ * reference).  For every detected photon with arrival time t (ns, as in the
+ * first-hit times), tc = min(max(t, 0), CL_MOMENT_T_MAX_NS) and
+ *   d_tsum [slot] += round(tc * CL_MOMENT_T_SCALE)
+ *   d_tsum2[slot] += round(fl(tc * tc) * CL_MOMENT_T2_SCALE)
+ * (Float32 products, round to nearest even; slot as in d_maps), so the sums
+ * are exact integers independent of the order of the photons.  They cannot
+ * overflow below about 1.6e7 detections per slot. */
+#define CL_MOMENT_T_SCALE 1048576.0f    /* 2^20 per ns */
+#define CL_MOMENT_T2_SCALE 65536.0f     /* 2^16 per ns^2 */
+#define CL_MOMENT_T_MAX_NS 4096.0f
+int cl_run_segments_moments_device(cl_handle* h,
+                                   const cl_box* box, const cl_optical_params* op,
+                                   const cl_readout* ro, const cl_time_binning* tb,
+                                   const float* d_sx, const float* d_sy, const float* d_sz,
+                                   const float* d_st, const int64_t* d_src_offsets,
+                                   const int32_t* d_src_segment, int64_t n_src,
+                                   int64_t n_segments, int64_t n_photons,
+                                   uint64_t seed, uint64_t pid_offset,
+                                   float tau_ns, int32_t max_bounces,
+                                   uint32_t* d_maps, float* d_tmin, int32_t* d_npe,
+                                   cl_counters* d_counters, uint64_t* d_tsum, uint64_t* d_tsum2,
+                                   void* stream);
+
 /* Wait for the work enqueued by the *_device calls on `stream` (NULL = the
  * handle's stream) and report device-side errors (CL_ERR_TIMEOUT). */
 int cl_sync(cl_handle* h, void* stream);
@@ -289,6 +314,8 @@ int cl_mlp_param_count(void);
 int cl_mlp_create(cl_mlp** out, int device, int max_batch);
 void cl_mlp_destroy(cl_mlp* m);
 const char* cl_mlp_last_error(const cl_mlp* m);
+/* Cap the CTAs of the batch-tiled GEMMs (0 = one per SM), for tests. */
+int cl_mlp_set_max_ctas(cl_mlp* m, int n);
 /* Host buffers of cl_mlp_param_count() floats; setting resets Adam's state. */
 int cl_mlp_set_params(cl_mlp* m, const float* host);
 int cl_mlp_get_params(cl_mlp* m, float* host);

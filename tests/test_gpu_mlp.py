@@ -56,6 +56,35 @@ def test_gradients_match_oracle(mlp):
         o += n
 
 
+@pytest.mark.parametrize("B,ctas", [(4096, 5), (2048, 3), (65536, 0)])
+def test_gradients_persistent_tiles(B, ctas):
+    """Few CTAs walking many 128-row tiles: exercises the stage ring across
+    tiles and both TMEM accumulators being reused."""
+    import torch
+    from crysplight_b200.surrogate import MLP
+    from oracle import mlp_oracle
+    from oracle.mlp_oracle import SHAPES
+    m = MLP(0, max_batch=B, seed=8)
+    m.set_max_ctas(ctas)      # 0: one CTA per SM; 65536 rows = the training batch, 64 K-splits
+    x, t = _batch(B, 4)
+    p = m.get_params().astype(np.float64)
+    loss, g = m.gradient(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda())
+    out = m.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    m.close()
+    rloss, rg = mlp_oracle.gradient(p, x, t)
+    ref, _ = mlp_oracle.forward(p, x)
+    assert np.abs(out - ref).max() < 2e-3 * max(1.0, np.abs(ref).max())
+    assert loss == pytest.approx(rloss, rel=1e-3)
+    o = 0
+    for name, shp in SHAPES:
+        n = int(np.prod(shp))
+        a, b = g[o:o + n].astype(np.float64), rg[o:o + n]
+        rel = float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30))
+        print(name, "rel", rel)
+        assert rel < 2e-3
+        o += n
+
+
 def test_training_reduces_loss():
     import torch
     from crysplight_b200.surrogate import MLP

@@ -28,6 +28,8 @@ def _gemm(lib, A, B, M, N, K, grid_x, splits):
     (512, 192, 128, 3, 1),
     (1024, 256, 256, 4, 1),
     (256, 256, 1024, 2, 4),
+    (2048, 256, 256, 3, 1),      # 16 tiles over 3 CTAs: both accumulators reused
+    (2560, 192, 192, 2, 1),
 ])
 def test_umma_gemm_matches_torch(M, N, K, grid_x, splits):
     import torch
