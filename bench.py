@@ -118,6 +118,107 @@ def run_events_bench(eng, E, steps: int, warmup: int, dev, stream, pid_base: int
                 d2h=int(2 * 4 * 64 * n_seg + 4 * n_seg + 72 + 12))
 
 
+SURROGATE_BGO = os.path.join(ROOT, "crysplight_b200", "surrogates", "bgo_esr.npz")
+
+
+def surrogate_events_workload(n_events: int = 500_000):
+    """Config 5: 511 keV gammas on BGO + ESR (geometry of runs/gammas_bgo_500k.toml,
+    48x48x22.4 mm, PDE 0.40, 100 ns x 120 bins; seed 99, yield 14000/MeV,
+    tau 1768 ns, density 7.13 g/cm3)."""
+    from crysplight_b200.params import (Box, OpticalParams, Readout, SipmGrid, TimeBinning,
+                                        deg2rad_f32)
+    from crysplight_b200.events import GammaMaterial
+    box = Box((48.0, 48.0, 22.4))
+    op = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, deg2rad_f32(1.3), 0.40)
+    return dict(name="events_bgo_surrogate", box=box, op=op, ro=Readout(SipmGrid(6.0, 8, 8)),
+                tb=TimeBinning(100.0, 120), tau=1768.0, seed=99, yield_=14_000.0,
+                mat=GammaMaterial.from_csv("BGO", 7.13, "xcom_BGO.csv"), n_events=n_events,
+                desc=f"{n_events} 511 keV gammas, BGO+ESR 48x48x22.4 mm, PDE 0.40, surrogate "
+                     "light maps with Monte Carlo fallback (ensemble spread > 2% or < 1 mm "
+                     "from a wrapped face)")
+
+
+def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wall_min_mm=1.0):
+    """events/s of the surrogate + fallback pipeline with the deposits in HBM
+    (value), the plain Monte Carlo on the same deposits, their agreement, and
+    the whole public call SurrogateEvents.run_events (e2e)."""
+    import torch
+    from crysplight_b200.events import gamma_stage
+    from crysplight_b200.fast_events import SurrogateEvents, compare_maps, photopeak
+    from crysplight_b200.surrogate import LightSurrogate
+    sur = LightSurrogate.load(SURROGATE_BGO)
+    se = SurrogateEvents(sur, eng, device=dev.index or 0)
+    g = gamma_stage(E["mat"], E["box"], n_events=E["n_events"], seed=E["seed"],
+                    yield_per_mev=E["yield_"])
+    nd = g.dep_photons.size
+    n_seg = E["n_events"]
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    xyz, t0, ph, seg = T(g.dep_xyz), T(g.dep_t), T(g.dep_photons), T(g.dep_event)
+    sptr = stream.cuda_stream
+    kw = dict(xyz=xyz, t0=t0, photons=ph, segment=seg, n_segments=n_seg, seed=E["seed"],
+              tau_ns=E["tau"], wall_min_mm=wall_min_mm, stream=sptr)
+
+    def step():
+        return se.transport_sites(E["box"], E["op"], E["ro"], E["tb"], **kw)
+    for _ in range(warmup):
+        step()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    times, out = [], None
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out = step()
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b) * 1e-3)
+    (maps, tmin, npe, ctr, sampled), stats = out
+    dev_s = sum(times) / steps
+    s_maps = maps.cpu().numpy().view(np.uint32).reshape(n_seg, 64)
+    s_npe = npe.cpu().numpy()
+    # the plain Monte Carlo of every deposit
+    off = np.zeros(nd + 1, np.int64)
+    np.cumsum(g.dep_photons, out=off[1:])
+    d_off = T(off)
+    m_maps = torch.empty(64 * n_seg, dtype=torch.int32, device=dev)
+    m_tmin = torch.empty(64 * n_seg, dtype=torch.float32, device=dev)
+    m_npe = torch.empty(n_seg, dtype=torch.int32, device=dev)
+    m_ctr = torch.empty(9, dtype=torch.int64, device=dev)
+    xs = [xyz[:, i].contiguous() for i in range(3)]
+    flush.zero_()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    eng.run_segments_device(E["box"], E["op"], E["ro"], E["tb"], sx=xs[0].data_ptr(),
+                            sy=xs[1].data_ptr(), sz=xs[2].data_ptr(), st=t0.data_ptr(),
+                            src_offsets=d_off.data_ptr(), src_segment=seg.data_ptr(), n_src=nd,
+                            n_segments=n_seg, n_photons=int(off[-1]), seed=E["seed"] + 1,
+                            pid_offset=0, tau_ns=E["tau"], maps=m_maps.data_ptr(),
+                            tmin=m_tmin.data_ptr(), npe=m_npe.data_ptr(), counters=m_ctr.data_ptr(),
+                            stream=sptr)
+    b.record(stream)
+    eng.sync(sptr)
+    mc_s = a.elapsed_time(b) * 1e-3
+    mc_steps = eng.last_steps
+    mm = m_maps.cpu().numpy().view(np.uint32).reshape(n_seg, 64)
+    pk_s, pk_m = photopeak(s_npe, g.edep), photopeak(m_npe.cpu().numpy(), g.edep)
+    cmp = compare_maps(s_maps.T.reshape(8, 8, n_seg), mm.T.reshape(8, 8, n_seg))
+    # end to end: the public call (host gamma stage, copies in, maps out)
+    se.run_events(E["box"], E["op"], E["ro"], E["tb"], E["mat"], E["yield_"], n_events=n_seg,
+                  seed=E["seed"], tau_ns=E["tau"], wall_min_mm=wall_min_mm)
+    t_e2e = time.perf_counter()
+    for _ in range(steps):
+        se.run_events(E["box"], E["op"], E["ro"], E["tb"], E["mat"], E["yield_"], n_events=n_seg,
+                      seed=E["seed"], tau_ns=E["tau"], wall_min_mm=wall_min_mm)
+    e2e_s = (time.perf_counter() - t_e2e) / steps
+    se.close()
+    return dict(value=n_seg / dev_s, e2e=n_seg / e2e_s, dev_s=dev_s, mc_value=n_seg / mc_s,
+                mc_s=mc_s, mc_photon_steps=mc_steps, photons=int(off[-1]), deposits=nd,
+                members=len(sur.members),
+                stats=stats, photopeak_surrogate=pk_s, photopeak_mc=pk_m,
+                photopeak_shift=(pk_s["mean"] - pk_m["mean"]) / pk_m["mean"], maps=cmp,
+                h2d=int(12 * nd + 4 * nd + 8 * nd + 4 * nd), d2h=int(2 * 4 * 64 * n_seg + 4 * n_seg + 72 + 16 + nd))
+
+
 def events_cpu_baseline(E, target_s: float) -> dict:
     """The oracle transports the photons of a sample of events (after the host
     gamma stage) on all host threads: events/s."""
@@ -472,7 +573,7 @@ def run_events_arm(args, rank, world, local_rank):
     import crysplight_b200 as cl
     if rank != 0 and args.impl == "reference":
         return
-    E = events_workload(args.n_events)
+    E = events_workload(args.n_events or 50_000)
     if args.impl == "reference":
         base = events_cpu_baseline(E, args.cpu_seconds)
         for _ in range(args.warmup):
@@ -524,19 +625,85 @@ def run_events_arm(args, rank, world, local_rank):
     eng.close()
 
 
+def run_surrogate_events_arm(args, rank, world, local_rank):
+    """--workload events_bgo_surrogate: events/s of the surrogate + Monte Carlo
+    fallback pipeline (config 5), the plain CUDA Monte Carlo on the same events,
+    and their agreement (photopeak, per-SiPM chi2)."""
+    import torch
+    import crysplight_b200 as cl
+    E = surrogate_events_workload(args.n_events or 500_000)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = events_cpu_baseline(E, args.cpu_seconds)
+        line = {"impl": "reference", "metric": "511keV events/s", "value": base["value"],
+                "unit": "events/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * E["n_events"] / base["value"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": E["name"], "desc": E["desc"]}, "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": "events/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    eng = cl.Engine(local_rank)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    r = run_surrogate_events_bench(eng, E, args.steps, args.warmup, dev, stream,
+                                   wall_min_mm=args.wall_min_mm)
+    clk = clocks.stop()
+    dev_s, e2e_s = r["dev_s"], E["n_events"] / r["e2e"]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s, e2e_s = float(t[0]), float(t[1])
+    if rank == 0:
+        line = {"metric": "511keV events/s", "value": world * E["n_events"] / dev_s,
+                "unit": "events/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": dev_s * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+bf16", "data": "synthetic",
+                "config": {"workload": E["name"], "desc": E["desc"], "deposits": r["deposits"],
+                           "photons_per_step": r["photons"], "wall_min_mm": args.wall_min_mm,
+                           "l2": "flushed between timed steps (256 MiB memset)"},
+                "e2e": {"value": world * E["n_events"] / e2e_s, "unit": "events/s",
+                        "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+                # per step: K members x 65536-row chunks x (layer 1 + 3 tcgen05 GEMMs),
+                # the ensemble combine, init + transport + sampler + finalize
+                "gpu_launches": args.steps * (r["members"] * -(-r["deposits"] // 65536) * 4 + 5),
+                "plain_mc": {"value": r["mc_value"], "unit": "events/s", "seconds": r["mc_s"],
+                             "photon_steps": r["mc_photon_steps"]},
+                "speedup_vs_plain_mc": r["value"] / r["mc_value"],
+                "sites": r["stats"], "photopeak_surrogate": r["photopeak_surrogate"],
+                "photopeak_mc": r["photopeak_mc"], "photopeak_shift": r["photopeak_shift"],
+                "maps_vs_mc": r["maps"], "clocks": clk}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = events_cpu_baseline(E, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
-    ap.add_argument("--workload", choices=("scan256", "point1m", "events_csitl"),
+    ap.add_argument("--workload", choices=("scan256", "point1m", "events_csitl",
+                                           "events_bgo_surrogate"),
                     default="scan256")
     ap.add_argument("--events", type=int, default=10_000,
                     help="events in the secondary events/s measurement of the default run "
                          "(0 = skip)")
-    ap.add_argument("--n-events", type=int, default=50_000,
-                    help="events of --workload events_csitl")
+    ap.add_argument("--n-events", type=int, default=0,
+                    help="events of --workload events_csitl (default 50000) or "
+                         "events_bgo_surrogate (default 500000)")
+    ap.add_argument("--wall-min-mm", type=float, default=1.0,
+                    help="events_bgo_surrogate: sites closer than this to a wrapped face "
+                         "go to the Monte Carlo")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=256,
@@ -548,6 +715,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "events_bgo_surrogate":
+        run_surrogate_events_arm(args, rank, world, local_rank)
+        return
     if args.workload == "events_csitl":
         if world > 1 and args.impl == "cuda":
             import datetime

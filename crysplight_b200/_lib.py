@@ -21,6 +21,7 @@ EXPORTS = (
     "cl_run_photons", "cl_run_photons_device", "cl_run_segments",
     "cl_run_segments_device", "cl_sync", "cl_last_steps", "cl_set_launch",
     "cl_debug_eval", "cl_run_photons_noalloc", "cl_run_segments_moments_device",
+    "cl_run_events_surrogate_device", "cl_surrogate_combine", "cl_debug_sampler",
 )
 
 # Fixed-point scales of cl_run_segments_moments_device (crysplight_cuda.h)
@@ -96,6 +97,16 @@ def _declare(lib: C.CDLL) -> None:
         _P, _P, _P, _P, C.c_int32, C.c_int64, C.c_uint64, C.c_uint64, C.c_float, C.c_int32,
         _P, _P, C.POINTER(Counters), _P]
     lib.cl_run_photons_noalloc.restype = C.c_int
+    lib.cl_run_events_surrogate_device.argtypes = common + [
+        _P, _P, _P, _P, _P, _P, C.c_int64, C.c_int64, C.c_uint64, C.c_uint64, C.c_float, C.c_int32,
+        _P, _P, _P, _P, _P, _P, _P, C.c_int64, C.c_uint64, C.c_int64, _P, _P, _P, _P, _P, _P]
+    lib.cl_run_events_surrogate_device.restype = C.c_int
+    lib.cl_surrogate_combine.argtypes = [_P, C.c_int32, C.c_int64, _P, _P, _P, C.POINTER(Box),
+                                         C.POINTER(Readout), C.c_float, C.c_float, C.c_float,
+                                         _P, _P, _P, _P, _P, _P]
+    lib.cl_surrogate_combine.restype = C.c_int
+    lib.cl_debug_sampler.argtypes = [C.c_int, _P, C.c_int64, C.c_uint64, _P, _P, _P]
+    lib.cl_debug_sampler.restype = C.c_int
 
 
 def load() -> C.CDLL:

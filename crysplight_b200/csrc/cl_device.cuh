@@ -153,8 +153,8 @@ __device__ __forceinline__ float simple_randu(SimpleStream& s, uint32_t k0, uint
 
 // Out-of-domain arguments (never reached by the transport): CUDA's Float64
 // functions, kept out of line so the hot loop stays small.
-__device__ __noinline__ float slow_logf(float x) { return __double2float_rn(log((double)x)); }
-__device__ __noinline__ float2 slow_sincosf(float x)
+static __device__ __noinline__ float slow_logf(float x) { return __double2float_rn(log((double)x)); }
+static __device__ __noinline__ float2 slow_sincosf(float x)
 {
     const double xd = (double)x;
     return make_float2(__double2float_rn(sin(xd)), __double2float_rn(cos(xd)));

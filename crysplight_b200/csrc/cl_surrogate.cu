@@ -1,0 +1,406 @@
+// cl_surrogate.cu — events from the learned light-response surrogate.
+//
+// The surrogate (cl_mlp.cu) maps an emission point to, per SiPM, the
+// probability that a photon emitted there is detected by that SiPM and the
+// mean and log standard deviation of the detected photons' transit times.
+// For a 511 keV event the deposits ("sites") that the surrogate can be
+// trusted with are sampled here instead of transported:
+//
+//   * surrogate_combine: the K ensemble members' outputs -> ensemble-mean
+//     probabilities (times the PDE), transit-time mean and sigma, the members'
+//     relative spread, and a fallback flag (spread above a threshold, the
+//     site within a distance of a wrapped face, or detection probabilities
+//     summing to 1 or more) that sends the site to the plain Monte Carlo;
+//   * surrogate_sample: per unflagged site, the N emitted photons are split
+//     over the SiPMs multinomially by a chain of conditional binomial draws
+//     (n_j ~ Bin(N - sum_{i<j} n_i, p_j / (1 - sum_{i<j} p_i))), and each
+//     SiPM's first-hit time is drawn exactly as the minimum of its n_j arrival
+//     times, each an exponential emission delay (decay time tau) plus a
+//     Gaussian transit time: the minimum's CDF is 1 - (1 - F)^n_j with F the
+//     exponentially modified Gaussian CDF, inverted by safeguarded Newton.
+//
+// Binomial variates: inversion for n*p < 10, otherwise Hormann's BTRD
+// (W. Hormann, "The generation of binomial random variates", J. Statist.
+// Comput. Simul. 46 (1993) 101-110), both in Float64.  Uniforms come from
+// Philox4x32-10 keyed with the event seed, counter (site lo, site hi, block,
+// 0x53555247): a stream domain disjoint from the transport's photon streams
+// (whose fourth counter word is 0).
+//
+// Every loop is bounded; a budget that runs out sets bit 2 of the error word
+// and the site's remaining draws fall back to the mean.
+#include <cmath>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "../../include/crysplight_cuda.h"
+#include "cl_device.cuh"
+#include "cl_surrogate.cuh"
+
+namespace cl {
+namespace sur {
+
+constexpr uint32_t STREAM_TAG = 0x53555247u;   // "SURG"
+constexpr unsigned SAMPLER_BUDGET_BIT = 4u;
+
+// Float64 uniforms in (0, 1) from one Philox stream.
+struct Uni {
+    uint32_t lo, hi, block, k0, k1;
+    uint32_t buf[4];
+    int left;
+    __device__ void init(uint64_t stream, uint32_t key0, uint32_t key1)
+    {
+        lo = (uint32_t)stream; hi = (uint32_t)(stream >> 32); block = 0; k0 = key0; k1 = key1; left = 0;
+    }
+    __device__ double next()
+    {
+        if (left == 0) {
+            const uint4 o = philox4x32_10(make_uint4(lo, hi, block, STREAM_TAG), k0, k1);
+            block += 1u;
+            buf[0] = o.x; buf[1] = o.y; buf[2] = o.z; buf[3] = o.w;
+            left = 4;
+        }
+        const uint32_t x = buf[4 - left];
+        left -= 1;
+        return ((double)x + 0.5) * 0x1p-32;
+    }
+};
+
+// Stirling-series remainder fc(k) = log(k!) - [(k + 1/2) log(k + 1) - (k + 1) + log(2 pi)/2].
+__device__ double stirling_fc(int64_t k)
+{
+    const double N = (double)k + 1.0;
+    if (k < 10) return lgamma(N) - (N - 0.5) * log(N) + N - 0.91893853320467274178;
+    const double r = 1.0 / N, r2 = r * r;
+    return (1.0 / 12.0 - (1.0 / 360.0 - (1.0 / 1260.0) * r2) * r2) * r;
+}
+
+// Inversion, n * p < 10, p <= 1/2 (sequential search from 0).
+__device__ int64_t binom_inversion(int64_t n, double p, Uni& U, unsigned& bad)
+{
+    const double q = 1.0 - p, s = p / q, a = (double)(n + 1) * s;
+    const double r0 = exp((double)n * log1p(-p));
+    for (int attempt = 0; attempt < 64; ++attempt) {
+        double u = U.next(), r = r0;
+        int64_t x = 0;
+        for (;;) {
+            if (u <= r) return x;
+            u -= r;
+            ++x;
+            if (x > n || x > 200) break;        // round-off tail: draw again
+            r *= a / (double)x - s;
+        }
+    }
+    bad |= SAMPLER_BUDGET_BIT;
+    return (int64_t)((double)n * p + 0.5);
+}
+
+// BTRD, n * p >= 10, p <= 1/2.
+__device__ int64_t binom_btrd(int64_t n, double p, Uni& U, unsigned& bad)
+{
+    const double q = 1.0 - p;
+    const double np = (double)n * p, npq = np * q, spq = sqrt(npq);
+    const int64_t m = (int64_t)floor((double)(n + 1) * p);
+    const double r = p / q, nr = (double)(n + 1) * r;
+    const double b = 1.15 + 2.53 * spq;
+    const double a = -0.0873 + 0.0248 * b + 0.01 * p;
+    const double c = np + 0.5;
+    const double alpha = (2.83 + 5.1 / b) * spq;
+    const double vr = 0.92 - 4.2 / b;
+    const double urvr = 0.86 * vr;
+    for (int it = 0; it < 1000; ++it) {
+        double v = U.next(), u;
+        if (v <= urvr) {
+            u = v / vr - 0.43;
+            return (int64_t)floor((2.0 * a / (0.5 - fabs(u)) + b) * u + c);
+        }
+        if (v >= vr) {
+            u = U.next() - 0.5;
+        } else {
+            u = v / vr - 0.93;
+            u = copysign(0.5, u) - u;
+            v = U.next() * vr;
+        }
+        const double us = 0.5 - fabs(u);
+        const double kd = floor((2.0 * a / us + b) * u + c);
+        if (kd < 0.0 || kd > (double)n) continue;
+        const int64_t k = (int64_t)kd;
+        v = v * alpha / (a / (us * us) + b);
+        const int64_t km = k > m ? k - m : m - k;
+        if (km <= 15) {
+            double f = 1.0;
+            if (m < k) {
+                for (int64_t i = m + 1; i <= k; ++i) f *= nr / (double)i - r;
+            } else if (m > k) {
+                for (int64_t i = k + 1; i <= m; ++i) v *= nr / (double)i - r;
+            }
+            if (v <= f) return k;
+            continue;
+        }
+        v = log(v);
+        const double kmd = (double)km;
+        const double rho = (kmd / npq) * (((kmd / 3.0 + 0.625) * kmd + 1.0 / 6.0) / npq + 0.5);
+        const double t = -kmd * kmd / (2.0 * npq);
+        if (v < t - rho) return k;
+        if (v > t + rho) continue;
+        const double nm = (double)(n - m + 1);
+        const double h = ((double)m + 0.5) * log(((double)m + 1.0) / (r * nm)) + stirling_fc(m) +
+                         stirling_fc(n - m);
+        const double nk = (double)(n - k + 1);
+        if (v <= h + (double)(n + 1) * log(nm / nk) + ((double)k + 0.5) * log(nk * r / ((double)k + 1.0)) -
+                     stirling_fc(k) - stirling_fc(n - k))
+            return k;
+    }
+    bad |= SAMPLER_BUDGET_BIT;
+    return (int64_t)(np + 0.5);
+}
+
+__device__ int64_t binomial(int64_t n, double p, Uni& U, unsigned& bad)
+{
+    if (n <= 0 || !(p > 0.0)) return 0;
+    if (p >= 1.0) return n;
+    const bool flip = p > 0.5;
+    const double pp = flip ? 1.0 - p : p;
+    const int64_t k = ((double)n * pp < 10.0) ? binom_inversion(n, pp, U, bad) : binom_btrd(n, pp, U, bad);
+    return flip ? n - k : k;
+}
+
+// Exponentially modified Gaussian: X = E + T, E ~ Exp(rate lam), T ~ N(mu, sigma^2),
+// in the standardised variable z = (t - mu) / sigma with ls = lam * sigma.
+// Returns F(t) and sets *dens to the density f(t).
+// Both terms carry exp(-z^2/2) where it would otherwise under/overflow
+// (erfcx(x) = exp(x^2) erfc(x)).
+__device__ double emg_cdf(double z, double ls, double lam, double* dens)
+{
+    constexpr double R2 = 0.70710678118654752440;
+    const double w = z - ls;
+    double phi_z, term2;
+    if (w < 0.0) {
+        term2 = 0.5 * exp(-0.5 * z * z) * erfcx(-w * R2);
+    } else {
+        term2 = 0.5 * exp(-ls * z + 0.5 * ls * ls) * erfc(-w * R2);
+    }
+    if (z < 0.0) phi_z = 0.5 * exp(-0.5 * z * z) * erfcx(-z * R2);
+    else phi_z = 0.5 * erfc(-z * R2);
+    *dens = lam * term2;            // density per unit t
+    return phi_z - term2;
+}
+
+// Minimum of k >= 1 independent EMG(mu, sigma, tau) arrival times, by
+// inverting P(min <= t) = 1 - (1 - F(t))^k at one uniform.
+__device__ double emg_min(int64_t k, double mu, double sigma, double tau, Uni& U, unsigned& bad)
+{
+    const double u = U.next();
+    const double lu = log(u) / (double)k;       // log of the survival level, < 0
+    const double y = -expm1(lu);                // target F(t) in (0, 1)
+    if (!(tau > 0.0)) return mu + sigma * normcdfinv(y);
+    if (!(sigma > 0.0)) return mu - tau * lu;   // pure exponential: F = 1 - exp(-(t - mu)/tau)
+    const double lam = 1.0 / tau, ls = lam * sigma;
+    // bracket in z: F(lo) < y <= F(hi)
+    double lo = -40.0, hi = 12.0 + (-tau * lu) / sigma + 0.5 * tau / sigma;
+    double dens = 0.0;
+    for (int g = 0; g < 64 && emg_cdf(hi, ls, lam, &dens) < y; ++g) hi = 2.0 * hi + 1.0;
+    double z = fmin(fmax((-tau * lu) / sigma, lo), hi);
+    for (int it = 0; it < 100; ++it) {
+        const double F = emg_cdf(z, ls, lam, &dens) - y;
+        if (F < 0.0) lo = z; else hi = z;
+        const double fz = dens * sigma;            // dF/dz
+        double zn = (fz > 0.0) ? z - F / fz : 0.5 * (lo + hi);
+        if (!(zn > lo && zn < hi)) zn = 0.5 * (lo + hi);
+        if (fabs(zn - z) < 1e-9 * fmax(1.0, fabs(z)) || hi - lo < 1e-9 * fmax(1.0, fabs(z)))
+            return mu + sigma * zn;
+        z = zn;
+    }
+    bad |= SAMPLER_BUDGET_BIT;
+    return mu + sigma * z;
+}
+
+__global__ void __launch_bounds__(128) surrogate_sample(const SurSampleArgs A)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned bad = 0;
+    unsigned long long ph = 0, det = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+        if (A.flag && A.flag[i]) continue;
+        int64_t left = A.photons[i];
+        if (left <= 0) continue;
+        ph += (unsigned long long)left;
+        Uni U;
+        U.init((uint64_t)i, A.k0, A.k1);
+        const float* p = A.p + i * A.cells;
+        const float* tm = A.tmean + i * A.cells;
+        const float* ts = A.tsig + i * A.cells;
+        const double t0 = (double)A.t0[i];
+        const int64_t base = (int64_t)A.seg[i] * A.cells;
+        double mass = 1.0;                          // probability not yet assigned
+        for (int c = 0; c < A.cells && left > 0; ++c) {
+            const double pc = (double)p[c];
+            const double pcond = mass > 0.0 ? fmin(fmax(pc / mass, 0.0), 1.0) : 1.0;
+            mass -= pc;
+            const int64_t k = binomial(left, pcond, U, bad);
+            if (k <= 0) continue;
+            left -= k;
+            det += (unsigned long long)k;
+            atomicAdd(A.maps + base + c, (uint32_t)k);
+            const double t = emg_min(k, (double)tm[c], (double)ts[c], (double)A.tau, U, bad);
+            atomicMin(A.keys + base + c, float_key((float)(t0 + t)));
+        }
+    }
+    if (A.stats) {
+        // one pair of atomics per warp
+        for (int o = 16; o > 0; o >>= 1) {
+            ph += __shfl_down_sync(0xffffffffu, ph, o);
+            det += __shfl_down_sync(0xffffffffu, det, o);
+        }
+        if ((threadIdx.x & 31) == 0 && (ph | det)) {
+            atomicAdd(A.stats, ph);
+            atomicAdd(A.stats + 1, det);
+        }
+    }
+    if (bad) atomicOr(A.err, bad);
+}
+
+// Ensemble reduction: 64 threads per site (one per SiPM), 4 sites per CTA.
+struct CombineArgs {
+    const float* raw;        // [K][n][3 * cells] standardised member outputs
+    int32_t K;
+    int64_t n;
+    const float* y_mean;     // [3 * cells]
+    const float* y_std;      // [3 * cells]
+    const float* xyz;        // [n][3] mm
+    float L0, L1, L2;
+    int32_t front_wrapped;
+    float pde, spread_max, wall_min_mm;
+    float* p;
+    float* tmean;
+    float* tsig;
+    float* spread;
+    uint8_t* flag;
+};
+
+constexpr int CELLS = 64;
+constexpr int SITES_PER_CTA = 4;
+
+__global__ void __launch_bounds__(CELLS * SITES_PER_CTA) surrogate_combine(const CombineArgs A)
+{
+    __shared__ double red[SITES_PER_CTA][2][2];
+    const int c = threadIdx.x % CELLS;
+    const int s_loc = threadIdx.x / CELLS;
+    const int warp_in_site = c / 32;
+    const float mp = A.y_mean[c], sp = A.y_std[c];
+    const float mt = A.y_mean[CELLS + c], st = A.y_std[CELLS + c];
+    const float ml = A.y_mean[2 * CELLS + c], sl = A.y_std[2 * CELLS + c];
+    for (int64_t s0 = (int64_t)blockIdx.x * SITES_PER_CTA; s0 < A.n; s0 += (int64_t)gridDim.x * SITES_PER_CTA) {
+        const int64_t i = s0 + s_loc;
+        double sum_p = 0.0, sum_p2 = 0.0, sum_t = 0.0, sum_l = 0.0;
+        if (i < A.n) {
+            for (int k = 0; k < A.K; ++k) {
+                const float* row = A.raw + ((int64_t)k * A.n + i) * (3 * CELLS);
+                const double pk = exp((double)row[c] * sp + mp);
+                sum_p += pk;
+                sum_p2 += pk * pk;
+                sum_t += (double)row[CELLS + c] * st + mt;
+                sum_l += (double)row[2 * CELLS + c] * sl + ml;
+            }
+        }
+        const double invK = 1.0 / (double)A.K;
+        const double pm = sum_p * invK;
+        const double var = fmax(sum_p2 * invK - pm * pm, 0.0);
+        double a = sqrt(var), b = pm;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if ((c & 31) == 0) { red[s_loc][warp_in_site][0] = a; red[s_loc][warp_in_site][1] = b; }
+        __syncthreads();
+        if (i < A.n) {
+            A.p[i * CELLS + c] = (float)(pm * (double)A.pde);
+            A.tmean[i * CELLS + c] = (float)(sum_t * invK);
+            A.tsig[i * CELLS + c] = (float)exp(sum_l * invK);
+            if (c == 0) {
+                const double num = red[s_loc][0][0] + red[s_loc][1][0];
+                const double den = red[s_loc][0][1] + red[s_loc][1][1];
+                const float spr = (float)(num / fmax(den, 1e-30));
+                const float x = A.xyz[3 * i], y = A.xyz[3 * i + 1], z = A.xyz[3 * i + 2];
+                float d = fminf(fminf(x, A.L0 - x), fminf(y, A.L1 - y));
+                if (A.front_wrapped) d = fminf(d, z);
+                uint8_t f = 0;
+                if (!(spr <= A.spread_max)) f |= 1u;
+                if (d < A.wall_min_mm) f |= 2u;
+                if (!(den * (double)A.pde < 0.999)) f |= 4u;   // not a probability split: Monte Carlo
+                A.spread[i] = spr;
+                A.flag[i] = f;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Diagnostics: fn 0 = binomial(n = par[0], p = par[1]) -> int64,
+// fn 1 = emg_min(k = par[0], mu = par[1], sigma = par[2], tau = par[3]) -> double.
+__global__ void debug_sampler(int fn, double p0, double p1, double p2, double p3, int64_t n,
+                              uint32_t k0, uint32_t k1, void* out, unsigned int* err)
+{
+    unsigned bad = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        Uni U;
+        U.init((uint64_t)i, k0, k1);
+        if (fn == 0) ((int64_t*)out)[i] = binomial((int64_t)p0, p1, U, bad);
+        else ((double*)out)[i] = emg_min((int64_t)p0, p1, p2, p3, U, bad);
+    }
+    if (bad && err) atomicOr(err, bad);
+}
+
+}  // namespace sur
+
+cudaError_t launch_surrogate_sample(const SurSampleArgs& a, int num_sms, cudaStream_t st)
+{
+    if (a.n <= 0) return cudaSuccess;
+    const int64_t want = (a.n + 127) / 128;
+    const int64_t cap = (int64_t)num_sms * 16;
+    sur::surrogate_sample<<<(unsigned)(want < cap ? want : cap), 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace cl
+
+extern "C" {
+
+int cl_surrogate_combine(const float* d_raw, int32_t members, int64_t n_sites,
+                         const float* d_y_mean, const float* d_y_std, const float* d_xyz,
+                         const cl_box* box, const cl_readout* ro, float pde,
+                         float spread_max, float wall_min_mm,
+                         float* d_p, float* d_tmean, float* d_tsig, float* d_spread,
+                         uint8_t* d_flag, void* stream)
+{
+    if (!box || !ro || members < 1 || n_sites < 0) return CL_ERR_ARG;
+    if ((int64_t)ro->grid.nx * ro->grid.ny != cl::sur::CELLS) return CL_ERR_ARG;
+    if (n_sites == 0) return CL_OK;
+    if (!d_raw || !d_y_mean || !d_y_std || !d_xyz || !d_p || !d_tmean || !d_tsig || !d_spread || !d_flag)
+        return CL_ERR_ARG;
+    if (!(pde >= 0.0f && pde <= 1.0f)) return CL_ERR_ARG;
+    cl::sur::CombineArgs a;
+    a.raw = d_raw; a.K = members; a.n = n_sites; a.y_mean = d_y_mean; a.y_std = d_y_std; a.xyz = d_xyz;
+    a.L0 = box->L[0]; a.L1 = box->L[1]; a.L2 = box->L[2];
+    a.front_wrapped = ro->two_sided ? 0 : 1;
+    a.pde = pde; a.spread_max = spread_max; a.wall_min_mm = wall_min_mm;
+    a.p = d_p; a.tmean = d_tmean; a.tsig = d_tsig; a.spread = d_spread; a.flag = d_flag;
+    const int64_t want = (n_sites + cl::sur::SITES_PER_CTA - 1) / cl::sur::SITES_PER_CTA;
+    const unsigned grid = (unsigned)(want < 148 * 64 ? want : 148 * 64);
+    cl::sur::surrogate_combine<<<grid, cl::sur::CELLS * cl::sur::SITES_PER_CTA, 0, (cudaStream_t)stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
+}
+
+int cl_debug_sampler(int fn, const double* par, int64_t n, uint64_t seed, void* d_out,
+                     unsigned int* d_err, void* stream)
+{
+    if ((fn != 0 && fn != 1) || !par || n < 0 || (n > 0 && !d_out)) return CL_ERR_ARG;
+    if (n == 0) return CL_OK;
+    const unsigned grid = (unsigned)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+    cl::sur::debug_sampler<<<grid, 256, 0, (cudaStream_t)stream>>>(fn, par[0], par[1], par[2], par[3], n,
+                                                                   (uint32_t)seed, (uint32_t)(seed >> 32),
+                                                                   d_out, d_err);
+    return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -30,6 +30,7 @@
 
 #include "../../include/crysplight_cuda.h"
 #include "cl_device.cuh"
+#include "cl_surrogate.cuh"
 
 #define CL_VERSION_STRING "crysplight_b200 0.1.0 (sm_100a)"
 
@@ -948,7 +949,8 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
                             int64_t n_src, int64_t n_seg, int64_t n, uint64_t pid0,
                             uint32_t* maps, uint32_t* keys, int32_t* npe,
                             unsigned long long* counters, const cl_records* rec, cudaStream_t st,
-                            unsigned long long* tsum = nullptr, unsigned long long* tsum2 = nullptr)
+                            unsigned long long* tsum = nullptr, unsigned long long* tsum2 = nullptr,
+                            const SurSampleArgs* sample = nullptr)
 {
     const int cells = P.nx * P.ny;
     const int64_t total = (int64_t)cells * n_seg;
@@ -979,6 +981,11 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
                                 : launch_transport<1, false, false>(h, a, smem, st);
         if (rc != CL_OK) return rc;
     }
+    if (sample) {
+        SurSampleArgs sa = *sample;
+        sa.maps = maps; sa.keys = keys; sa.err = s.err;
+        CK(h, launch_surrogate_sample(sa, h->num_sms, st), "surrogate sampler launch");
+    }
     finalize_segments<<<(unsigned)std::min<int64_t>((total + 255) / 256 + 1, 8192), 256, 0, st>>>(
         maps, keys, npe, n_seg, cells);
     CK(h, cudaGetLastError(), "finalize launch");
@@ -995,6 +1002,7 @@ static int collect(cl_handle* h, cudaStream_t st)
     CK(h, cudaStreamSynchronize(st), "stream synchronize");
     h->last_steps = (int64_t)steps;
     if (err & 2u) return set_err(h, CL_ERR_CUDA, "internal error: uniform ring underflow in the transport kernel");
+    if (err & 4u) return set_err(h, CL_ERR_TIMEOUT, "a loop budget of the surrogate sampler ran out");
     if (err) return set_err(h, CL_ERR_TIMEOUT, "a device-side loop budget ran out (Rayleigh rejection sampler)");
     return CL_OK;
 }
@@ -1250,6 +1258,49 @@ int cl_run_segments_moments_device(cl_handle* h, const cl_box* box, const cl_opt
                             n_photons, pid_offset, d_maps, (uint32_t*)d_tmin, d_npe,
                             (unsigned long long*)d_counters, nullptr, st,
                             (unsigned long long*)d_tsum, (unsigned long long*)d_tsum2);
+}
+
+int cl_run_events_surrogate_device(cl_handle* h, const cl_box* box, const cl_optical_params* op,
+                                   const cl_readout* ro, const cl_time_binning* tb,
+                                   const float* d_sx, const float* d_sy, const float* d_sz,
+                                   const float* d_st, const int64_t* d_src_offsets,
+                                   const int32_t* d_src_segment, int64_t n_src, int64_t n_photons,
+                                   uint64_t seed, uint64_t pid_offset, float tau_ns, int32_t max_bounces,
+                                   const float* d_site_p, const float* d_site_tmean,
+                                   const float* d_site_tsig, const uint8_t* d_site_flag,
+                                   const float* d_site_t0, const int64_t* d_site_photons,
+                                   const int32_t* d_site_segment, int64_t n_sites, uint64_t sample_seed,
+                                   int64_t n_segments, uint32_t* d_maps, float* d_tmin, int32_t* d_npe,
+                                   cl_counters* d_counters, uint64_t* d_sampled, void* stream)
+{
+    if (!h) return CL_ERR_STATE;
+    h->err[0] = 0;
+    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    if (rc != CL_OK) return rc;
+    if (n_segments < 1) return set_err(h, CL_ERR_ARG, "need n_segments >= 1");
+    if (n_src < 0 || n_sites < 0 || n_photons < 0) return set_err(h, CL_ERR_ARG, "negative size");
+    if (n_src == 0 && n_photons != 0) return set_err(h, CL_ERR_ARG, "photons without Monte Carlo sources");
+    if (n_src > 0 && (!d_sx || !d_sy || !d_sz || !d_src_offsets || !d_src_segment))
+        return set_err(h, CL_ERR_ARG, "null source array");
+    if (n_sites > 0 && (!d_site_p || !d_site_tmean || !d_site_tsig || !d_site_t0 || !d_site_photons ||
+                        !d_site_segment))
+        return set_err(h, CL_ERR_ARG, "null surrogate site array");
+    if (!d_maps || !d_tmin || !d_npe || !d_counters) return set_err(h, CL_ERR_ARG, "null output buffer");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    SurSampleArgs sa;
+    memset(&sa, 0, sizeof sa);
+    sa.p = d_site_p; sa.tmean = d_site_tmean; sa.tsig = d_site_tsig; sa.flag = d_site_flag;
+    sa.t0 = d_site_t0; sa.photons = d_site_photons; sa.seg = d_site_segment; sa.n = n_sites;
+    sa.cells = ro->grid.nx * ro->grid.ny;
+    sa.k0 = (uint32_t)sample_seed; sa.k1 = (uint32_t)(sample_seed >> 32);
+    sa.tau = tau_ns;
+    sa.stats = (unsigned long long*)d_sampled;
+    if (d_sampled) CK(h, cudaMemsetAsync(d_sampled, 0, 2 * sizeof(uint64_t), st), "zero sampler stats");
+    const Physics P = make_physics(box, op, ro, tb, tau_ns, max_bounces, seed);
+    return enqueue_segments(h, P, d_sx, d_sy, d_sz, d_st, d_src_offsets, d_src_segment, n_src, n_segments,
+                            n_photons, pid_offset, d_maps, (uint32_t*)d_tmin, d_npe,
+                            (unsigned long long*)d_counters, nullptr, st, nullptr, nullptr, &sa);
 }
 
 int cl_sync(cl_handle* h, void* stream)

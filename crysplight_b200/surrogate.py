@@ -126,6 +126,11 @@ class MLP:
                                             x.shape[0]))
         return out
 
+    def forward_into(self, x, out) -> None:
+        """out[n][192] (float32 CUDA tensor, contiguous) = network(x[n][3])."""
+        self._check(self.lib.cl_mlp_forward(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()),
+                                            x.shape[0]))
+
     def gradient(self, x, t):
         g = np.empty(self.n_params, np.float32)
         loss = C.c_float()
@@ -262,13 +267,22 @@ class LightSurrogate:
 
     @classmethod
     def train(cls, box: Box, xyz: np.ndarray, targets: np.ndarray, *, members: int = 5, steps: int = 20000,
-              batch: int = 65536, lr: float = 1e-3, seed: int = 0, device: int = 0,
-              chunk: int = 500, log=None):
+              batch: int = 65536, lr: float = 1e-3, lr_final: Optional[float] = None,
+              time_weight: float = 1.0, seed: int = 0, device: int = 0, chunk: int = 250, log=None):
+        """Train ``members`` networks on standardised targets.
+
+        ``lr_final``: cosine decay of the Adam step size from ``lr`` to
+        ``lr_final`` over the steps (piecewise constant per ``chunk`` steps);
+        None keeps ``lr``.  ``time_weight``: weight of the 128 arrival-time
+        outputs in the squared-error loss relative to the 64 log-probabilities
+        (applied by standardising those targets with std / sqrt(time_weight))."""
+        import math
         import time
         import torch
         L = np.array([float(box.L[i]) for i in range(3)], np.float64)
         y_mean = targets.mean(0).astype(np.float64)
         y_std = np.maximum(targets.std(0), 1e-6).astype(np.float64)
+        y_std[N_CELLS:] /= math.sqrt(time_weight)
         obj = cls(L, y_mean.astype(np.float32), y_std.astype(np.float32), [])
         x = torch.from_numpy(obj.normalise(xyz)).to(f"cuda:{device}")
         y = torch.from_numpy(((targets - y_mean) / y_std).astype(np.float32)).to(f"cuda:{device}")
@@ -280,13 +294,19 @@ class LightSurrogate:
             hist = []
             for s0 in range(0, steps, chunk):
                 ns = min(chunk, steps - s0)
-                hist.append(net.train(ns, batch=batch, lr=lr, seed=seed * 1000 + k))
-                if log:
-                    log(f"member {k} step {s0 + ns}: loss {hist[-1]:.5f}")
+                if lr_final is None:
+                    lr_now = lr
+                else:
+                    mid = (s0 + 0.5 * ns) / steps
+                    lr_now = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * mid))
+                hist.append(net.train(ns, batch=batch, lr=lr_now, seed=seed * 1000 + k))
+                if log and ((s0 + ns) % 2000 == 0 or s0 + ns == steps):
+                    log(f"member {k} step {s0 + ns}: lr {lr_now:.2e} loss {hist[-1]:.5f}")
             obj.members.append(net.get_params())
             history.append(hist)
             net.close()
-        obj.meta = {"steps": steps, "batch": batch, "lr": lr, "seed": seed,
+        obj.meta = {"steps": steps, "batch": batch, "lr": lr, "lr_final": lr_final,
+                    "time_weight": time_weight, "seed": seed,
                     "train_seconds": time.perf_counter() - t0, "loss_history": history}
         return obj
 

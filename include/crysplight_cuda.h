@@ -258,6 +258,71 @@ int cl_run_segments_moments_device(cl_handle* h,
                                    cl_counters* d_counters, uint64_t* d_tsum, uint64_t* d_tsum2,
                                    void* stream);
 
+/*
+ * Events from the learned light-response surrogate with Monte Carlo fallback
+ * (no counterpart in the reference: it replaces, for the deposits the
+ * surrogate is trusted with, the transport that flush! (src/events.jl:65-91)
+ * launches through run_photons_ka!).  One call, all on `stream`:
+ *   1. the deposits that fell back to the Monte Carlo are transported exactly
+ *      as by cl_run_segments_device (same source, offset and segment arrays,
+ *      n_src may be 0);
+ *   2. every site i with d_site_flag[i] == 0 (d_site_flag may be NULL) splits
+ *      its d_site_photons[i] photons over the nx*ny SiPMs multinomially with
+ *      the per-photon detection probabilities d_site_p[i][cell] (conditional
+ *      binomial draws) and draws each hit SiPM's first-hit time as the minimum
+ *      of its photons' arrival times d_site_t0[i] + Exp(tau_ns) +
+ *      N(d_site_tmean, d_site_tsig^2); counts and times join segment
+ *      d_site_segment[i]'s map;
+ *   3. the maps' first times are decoded and npe summed, as in segment mode.
+ * Sampler uniforms: Philox4x32-10 keyed by sample_seed, a stream per site.
+ * d_counters count the Monte Carlo photons only; d_sampled (uint64[2], may be
+ * NULL) gets the photons of sampled sites and their sampled detections.
+ * Asynchronous; cl_sync reports CL_ERR_TIMEOUT if a sampler loop budget ran out.
+ */
+int cl_run_events_surrogate_device(cl_handle* h,
+                                   const cl_box* box, const cl_optical_params* op,
+                                   const cl_readout* ro, const cl_time_binning* tb,
+                                   const float* d_sx, const float* d_sy, const float* d_sz,
+                                   const float* d_st, const int64_t* d_src_offsets,
+                                   const int32_t* d_src_segment, int64_t n_src, int64_t n_photons,
+                                   uint64_t seed, uint64_t pid_offset, float tau_ns, int32_t max_bounces,
+                                   const float* d_site_p, const float* d_site_tmean,
+                                   const float* d_site_tsig, const uint8_t* d_site_flag,
+                                   const float* d_site_t0, const int64_t* d_site_photons,
+                                   const int32_t* d_site_segment, int64_t n_sites, uint64_t sample_seed,
+                                   int64_t n_segments, uint32_t* d_maps, float* d_tmin, int32_t* d_npe,
+                                   cl_counters* d_counters, uint64_t* d_sampled, void* stream);
+
+/*
+ * Ensemble reduction of the surrogate (no counterpart in the reference).
+ * d_raw [members][n_sites][3*64]: each member's standardised outputs
+ * (cl_mlp_forward); y = raw * d_y_std + d_y_mean gives per SiPM (64 = nx*ny,
+ * required) log detection probability, mean transit time (ns) and log of its
+ * standard deviation.  Writes per site and SiPM d_p = pde * mean_k exp(log p),
+ * d_tmean = mean_k, d_tsig = exp(mean_k log sigma); d_spread = sum over SiPMs
+ * of the members' standard deviation of p / sum of their mean p; d_flag bit 0:
+ * spread > spread_max, bit 1: the site (d_xyz [n][3] mm) lies closer than
+ * wall_min_mm to a wrapped face (the four side faces and, unless two-sided,
+ * the front face z = 0), bit 2: pde * sum of p >= 0.999.  Asynchronous on
+ * `stream`; allocates nothing.
+ */
+int cl_surrogate_combine(const float* d_raw, int32_t members, int64_t n_sites,
+                         const float* d_y_mean, const float* d_y_std, const float* d_xyz,
+                         const cl_box* box, const cl_readout* ro, float pde,
+                         float spread_max, float wall_min_mm,
+                         float* d_p, float* d_tmean, float* d_tsig, float* d_spread,
+                         uint8_t* d_flag, void* stream);
+
+/*
+ * Diagnostics for tests: n draws (stream i = draw i, key = seed) of the
+ * surrogate sampler's variates into device memory: fn 0 = binomial
+ * (n = par[0], p = par[1]) -> int64; fn 1 = minimum of k = par[0] arrival
+ * times Exp(tau = par[3]) + N(mu = par[1], sigma = par[2]^2) -> double.
+ * *d_err (device, may be NULL) gets bit 2 if a loop budget ran out.
+ */
+int cl_debug_sampler(int fn, const double* par, int64_t n, uint64_t seed, void* d_out,
+                     unsigned int* d_err, void* stream);
+
 /* Wait for the work enqueued by the *_device calls on `stream` (NULL = the
  * handle's stream) and report device-side errors (CL_ERR_TIMEOUT). */
 int cl_sync(cl_handle* h, void* stream);
