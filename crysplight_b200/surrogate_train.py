@@ -108,6 +108,8 @@ def main(argv=None):
     ap.add_argument("--out", required=True)
     ap.add_argument("--report", default=None)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--model", default=None,
+                    help="evaluate this trained ensemble (.npz) instead of training one")
     args = ap.parse_args(argv)
 
     from .surrogate import LightSurrogate, grid_points, light_targets, scan_light, split_holdout
@@ -127,13 +129,17 @@ def main(argv=None):
           f"({n_ph / scan.seconds / 1e6:.0f} M photons/s)", flush=True)
     y = light_targets(scan)
     tr, ho = split_holdout(pts.shape[0], 0.1, seed=11)
-    sur = LightSurrogate.train(box, pts[tr], y[tr], members=args.members, steps=args.steps, batch=args.batch,
-                               lr=args.lr, lr_final=args.lr_final if args.lr_final >= 0 else None,
-                               time_weight=args.time_weight, seed=args.seed, device=args.device,
-                               log=lambda s: print(s, flush=True))
-    rep["train_seconds"] = sur.meta["train_seconds"]
-    rep["final_loss"] = [h[-1] for h in sur.meta["loss_history"]]
-    print(f"training: {sur.meta['train_seconds']:.1f} s", flush=True)
+    if args.model:
+        sur = LightSurrogate.load(args.model)
+    else:
+        sur = LightSurrogate.train(box, pts[tr], y[tr], members=args.members, steps=args.steps,
+                                   batch=args.batch, lr=args.lr,
+                                   lr_final=args.lr_final if args.lr_final >= 0 else None,
+                                   time_weight=args.time_weight, seed=args.seed, device=args.device,
+                                   log=lambda s: print(s, flush=True))
+        rep["train_seconds"] = sur.meta["train_seconds"]
+        rep["final_loss"] = [h[-1] for h in sur.meta["loss_history"]]
+        print(f"training: {sur.meta['train_seconds']:.1f} s", flush=True)
 
     # held-out validation against a high-statistics truth
     rng = np.random.default_rng(5)
@@ -157,7 +163,33 @@ def main(argv=None):
         "spread_p95": float(np.quantile(pred["spread"], 0.95)),
         "truth_noise_mean": float(np.mean(np.sqrt(1.0 / np.maximum(truth.counts[p_true * args.photons > 100], 1)))),
     }
+    # the points the surrogate serves in event generation: at least 1 mm from a
+    # wrapped face (the four sides and the front face z = 0) and spread <= 2%
+    q = pts[sub].astype(np.float64)
+    L = [float(box.L[i]) for i in range(3)]
+    d_wall = np.minimum.reduce([q[:, 0], L[0] - q[:, 0], q[:, 1], L[1] - q[:, 1], q[:, 2]])
+    served = (d_wall >= 1.0) & (pred["spread"] <= 0.02)
+    rep["holdout"]["served_points"] = int(served.sum())
+    rep["holdout"]["surrogate_served"] = rel_error(pred["p"][served], p_true[served], args.photons)
+    rep["holdout"]["table_served"] = rel_error(p_tab[served], p_true[served], args.photons)
+    far = d_wall >= 1.0
+    rep["holdout"]["surrogate_wall_ge_1mm"] = rel_error(pred["p"][far], p_true[far], args.photons)
+    per_pt = np.array([rel_error(pred["p"][i:i + 1], p_true[i:i + 1], args.photons)["mean"]
+                       for i in range(sub.size)])
+    dz_read = L[2] - q[:, 2]
+    rep["holdout"]["by_distance_to_readout_mm"] = {
+        f"{lo}-{hi}": float(per_pt[(dz_read >= lo) & (dz_read < hi)].mean())
+        for lo, hi in ((0, 2), (2, 5), (5, 10), (10, 30)) if ((dz_read >= lo) & (dz_read < hi)).any()}
+    rep["holdout"]["by_distance_to_wall_mm"] = {
+        f"{lo}-{hi}": float(per_pt[(d_wall >= lo) & (d_wall < hi)].mean())
+        for lo, hi in ((0, 1), (1, 3), (3, 8), (8, 30)) if ((d_wall >= lo) & (d_wall < hi)).any()}
     print(json.dumps(rep["holdout"], indent=1), flush=True)
+    if args.model:
+        if args.report:
+            with open(args.report, "w") as f:
+                json.dump(rep, f, indent=1)
+        eng.close()
+        return rep
     sur.meta.update({"setup": args.setup, "grid": list(args.grid), "photons_per_point": args.photons})
     sur.save(args.out)
     if args.report:
