@@ -71,7 +71,10 @@ __device__ __forceinline__ float u32_to_randu(uint32_t x)
 // (every access is bank-conflict free).  Blocks are generated ahead of use, at
 // one convergent point of the warp loop; pop() consumes in order and peek(d)
 // looks d words ahead, so the sequence of uniforms is exactly the reference's.
-constexpr int RING_LEN = 16;
+#ifndef CL_RING_LEN
+#define CL_RING_LEN 28
+#endif
+constexpr int RING_LEN = CL_RING_LEN;
 constexpr int RING_STRIDE = 256;      // columns: the largest block the kernels launch
 
 struct Rng {
@@ -106,6 +109,26 @@ __device__ __forceinline__ void rng_fill2(Rng& r, float* ring, const uint32_t* r
     ring[((w + 6u) % RING_LEN) * RING_STRIDE] = u32_to_randu(q.z);
     ring[((w + 7u) % RING_LEN) * RING_STRIDE] = u32_to_randu(q.w);
     r.cnt += 8;
+}
+
+// NB consecutive blocks at once.  Requires cnt <= RING_LEN - 4 * NB.
+template <int NB>
+__device__ __forceinline__ void rng_fill(Rng& r, float* ring, const uint32_t* rk)
+{
+    uint4 o[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+        o[b] = philox4x32_10_rk(make_uint4(r.pid_lo, r.pid_hi, r.block + (uint32_t)b, 0u), rk);
+    r.block += (uint32_t)NB;
+    const uint32_t w = r.head + (uint32_t)r.cnt;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        ring[((w + 4u * b + 0u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o[b].x);
+        ring[((w + 4u * b + 1u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o[b].y);
+        ring[((w + 4u * b + 2u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o[b].z);
+        ring[((w + 4u * b + 3u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o[b].w);
+    }
+    r.cnt += 4 * NB;
 }
 
 __device__ __forceinline__ float rng_peek(const Rng& r, const float* ring, uint32_t d)

@@ -131,6 +131,12 @@ constexpr int DRAWS_PER_ITER = 7;
 // Fresnel interfaces met in an iteration (one evaluation serves all three).
 enum : int32_t { FK_NONE = 0, FK_READOUT = 1, FK_POLISHED = 2, FK_FACET = 3 };
 
+#ifndef CL_FILL_JOIN
+#define CL_FILL_JOIN 1
+#endif
+#ifndef CL_FILL_BLOCKS
+#define CL_FILL_BLOCKS 2
+#endif
 #ifndef CL_MIN_CTAS_PER_SM
 #define CL_MIN_CTAS_PER_SM 4
 #endif
@@ -240,7 +246,14 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
         {
             const bool want = st != S_IDLE && rng.cnt < DRAWS_PER_ITER;
             if (__any_sync(FULL, want)) {
+#if CL_FILL_JOIN
+                // every lane with room tops up at this convergent point, so
+                // later iterations need the fill less often
+                if (st != S_IDLE && rng.cnt <= RING_LEN - 4 * CL_FILL_BLOCKS)
+                    rng_fill<CL_FILL_BLOCKS>(rng, ring, P.rk);
+#else
                 if (want) rng_fill2(rng, ring, P.rk);
+#endif
             }
         }
 
@@ -720,11 +733,15 @@ static int ensure(cl_handle* h, DevBuf& b, size_t bytes)
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Allow dynamic shared memory up to the opt-in limit minus the kernel's
+// static shared memory (their sum may not exceed the limit).
 template <int MODE, bool REC, bool TILE>
 static void set_kernel_attrs(int smem_optin)
 {
-    cudaFuncSetAttribute(transport_kernel<MODE, REC, TILE>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, transport_kernel<MODE, REC, TILE>) != cudaSuccess) return;
+    cudaFuncSetAttribute(transport_kernel<MODE, REC, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         smem_optin - (int)fa.sharedSizeBytes);
 }
 
 extern "C" {
