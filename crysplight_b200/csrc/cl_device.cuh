@@ -121,6 +121,20 @@ __device__ __forceinline__ void rng_fill(Rng& r, float* ring, const uint32_t* rk
         o[b] = philox4x32_10_rk(make_uint4(r.pid_lo, r.pid_hi, r.block + (uint32_t)b, 0u), rk);
     r.block += (uint32_t)NB;
     const uint32_t w = r.head + (uint32_t)r.cnt;
+#if CL_RING_WRAP
+    // w < 2 RING_LEN: one conditional subtraction wraps each index
+    auto at = [&](uint32_t k) -> float& {
+        const uint32_t i = w + k;
+        return ring[(i >= (uint32_t)RING_LEN ? i - (uint32_t)RING_LEN : i) * RING_STRIDE];
+    };
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        at(4u * b + 0u) = u32_to_randu(o[b].x);
+        at(4u * b + 1u) = u32_to_randu(o[b].y);
+        at(4u * b + 2u) = u32_to_randu(o[b].z);
+        at(4u * b + 3u) = u32_to_randu(o[b].w);
+    }
+#else
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
         ring[((w + 4u * b + 0u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o[b].x);
@@ -128,20 +142,36 @@ __device__ __forceinline__ void rng_fill(Rng& r, float* ring, const uint32_t* rk
         ring[((w + 4u * b + 2u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o[b].z);
         ring[((w + 4u * b + 3u) % RING_LEN) * RING_STRIDE] = u32_to_randu(o[b].w);
     }
+#endif
     r.cnt += 4 * NB;
 }
 
+#ifndef CL_RING_WRAP
+#define CL_RING_WRAP 1
+#endif
+
 __device__ __forceinline__ float rng_peek(const Rng& r, const float* ring, uint32_t d)
 {
+#if CL_RING_WRAP
+    uint32_t i = r.head + d;                   // head < RING_LEN, d < RING_LEN
+    i = i >= (uint32_t)RING_LEN ? i - (uint32_t)RING_LEN : i;
+    return ring[i * RING_STRIDE];
+#else
     return ring[((r.head + d) % RING_LEN) * RING_STRIDE];
+#endif
 }
 
 // Pop the next uniform.  The warp loop keeps at least as many words buffered
 // as one iteration can consume (checked once per iteration through cnt).
 __device__ __forceinline__ float rng_pop(Rng& r, const float* ring)
 {
+#if CL_RING_WRAP
+    const float u = ring[r.head * RING_STRIDE];
+    r.head = r.head + 1u == (uint32_t)RING_LEN ? 0u : r.head + 1u;
+#else
     const float u = ring[(r.head % RING_LEN) * RING_STRIDE];
     r.head += 1u;
+#endif
     r.cnt -= 1;
     return u;
 }
@@ -186,6 +216,7 @@ static __device__ __noinline__ float2 slow_sincosf(float x)
 // Natural log.  Table-driven (Tang 1990): x = 2^e * m, m in [sqrt(1/2), sqrt(2)),
 // m = F_j (1 + r) with F_j = 1 + j/64, ln x = e ln2 + ln F_j + log1p(r),
 // |r| < 1/90, log1p by its Taylor series to r^8.
+template <int STRIDE = 1>
 __device__ __forceinline__ float cl_logf(float x, const double2* __restrict__ tab)
 {
     const uint32_t b = __float_as_uint(x);
@@ -199,7 +230,7 @@ __device__ __forceinline__ float cl_logf(float x, const double2* __restrict__ ta
     const double m = (double)__uint_as_float(mb);
     const int j = __double2int_rn((m - 1.0) * 64.0);
     const double F = 1.0 + (double)j * 0.015625;
-    const double2 t = tab[j - CLM_LOG_JMIN];
+    const double2 t = tab[(j - CLM_LOG_JMIN) * STRIDE];
     const double r = (m - F) * t.x;            // m - F is exact
     double p = CLM_L8;
     p = fma(p, r, CLM_L7);
@@ -215,6 +246,7 @@ __device__ __forceinline__ float cl_logf(float x, const double2* __restrict__ ta
 
 // log of a uniform ((x>>8)+1)*2^-24: always a positive normal float, so the
 // domain check of cl_logf is not needed.
+template <int STRIDE = 1>
 __device__ __forceinline__ float cl_logf_u(float x, const double2* __restrict__ tab)
 {
     const uint32_t b = __float_as_uint(x);
@@ -226,7 +258,7 @@ __device__ __forceinline__ float cl_logf_u(float x, const double2* __restrict__ 
     const double m = (double)__uint_as_float(mb);
     const int j = __double2int_rn((m - 1.0) * 64.0);
     const double F = 1.0 + (double)j * 0.015625;
-    const double2 t = tab[j - CLM_LOG_JMIN];
+    const double2 t = tab[(j - CLM_LOG_JMIN) * STRIDE];
     const double r = (m - F) * t.x;
     double p = CLM_L8;
     p = fma(p, r, CLM_L7);
@@ -246,6 +278,7 @@ __device__ __forceinline__ float cl_logf_u(float x, const double2* __restrict__ 
 // recombined as S + (S (cos r - 1) + C sin r) and C + (C (cos r - 1) - S sin r).
 // The table-driven core for 0 <= x <= 1e4 (the transport passes azimuths
 // 2*pi*u in (0, 2*pi] and facet tilts in [0, 1.2)); +0 maps to (+0, 1).
+template <int STRIDE = 1>
 __device__ __forceinline__ void cl_sincosf_core(float x, const double2* __restrict__ sctab,
                                                 float* sp, float* cp)
 {
@@ -253,7 +286,7 @@ __device__ __forceinline__ void cl_sincosf_core(float x, const double2* __restri
     const double n = rint(xd * CLM_SC_INV_DELTA);
     double r = fma(-n, CLM_SC_DELTA_HI, xd);
     r = fma(-n, CLM_SC_DELTA_LO, r);
-    const double2 sc = sctab[(int)n & (CLM_SC_N - 1)];
+    const double2 sc = sctab[((int)n & (CLM_SC_N - 1)) * STRIDE];
     const double r2 = r * r;
     double ps = fma(CLM_TS7, r2, CLM_TS5);
     ps = fma(ps, r2, CLM_TS3);
@@ -266,6 +299,7 @@ __device__ __forceinline__ void cl_sincosf_core(float x, const double2* __restri
     *cp = __double2float_rn(sc.y + fma(sc.y, cm1, -(sc.x * sr)));
 }
 
+template <int STRIDE = 1>
 __device__ __forceinline__ void cl_sincosf(float x, const double2* __restrict__ sctab,
                                            float* sp, float* cp)
 {
@@ -284,7 +318,7 @@ __device__ __forceinline__ void cl_sincosf(float x, const double2* __restrict__ 
     const double n = rint(xd * CLM_SC_INV_DELTA);
     double r = fma(-n, CLM_SC_DELTA_HI, xd);
     r = fma(-n, CLM_SC_DELTA_LO, r);
-    const double2 sc = sctab[(int)n & (CLM_SC_N - 1)];
+    const double2 sc = sctab[((int)n & (CLM_SC_N - 1)) * STRIDE];
     const double r2 = r * r;
     double ps = fma(CLM_TS7, r2, CLM_TS5);
     ps = fma(ps, r2, CLM_TS3);

@@ -37,8 +37,19 @@
 namespace cl {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int SCTAB_BYTES = CLM_SC_N * 16;
-constexpr int LOGTAB_BYTES = ((CLM_LOG_NTAB * 16 + 127) / 128) * 128 + SCTAB_BYTES;  // both tables
+// The tables are replicated: entry e of copy c sits at [e * COPIES + c] and a
+// lane reads copy (lane % COPIES), so the 16-byte reads of the 8 lanes that
+// share a shared-memory wavefront hit distinct banks when COPIES = 8.
+#ifndef CL_LOG_COPIES
+#define CL_LOG_COPIES 1
+#endif
+#ifndef CL_SC_COPIES
+#define CL_SC_COPIES 1
+#endif
+constexpr int LOG_COPIES = CL_LOG_COPIES;
+constexpr int SC_COPIES = CL_SC_COPIES;
+constexpr int SCTAB_BYTES = CLM_SC_N * 16 * SC_COPIES;
+constexpr int LOGTAB_BYTES = ((CLM_LOG_NTAB * 16 * LOG_COPIES + 127) / 128) * 128 + SCTAB_BYTES;  // both tables
 
 __constant__ double c_logtab[2 * CLM_LOG_NTAB] = { CLM_LOG_TAB_INIT };
 __constant__ double c_sctab[2 * CLM_SC_N] = { CLM_SC_TAB_INIT };
@@ -48,10 +59,14 @@ __device__ __forceinline__ void load_tables(unsigned char* smem, double2*& tab, 
 {
     sctab = reinterpret_cast<double2*>(smem);
     tab = reinterpret_cast<double2*>(smem + SCTAB_BYTES);
-    for (int i = threadIdx.x; i < CLM_SC_N; i += blockDim.x)
-        sctab[i] = make_double2(c_sctab[2 * i], c_sctab[2 * i + 1]);
-    for (int i = threadIdx.x; i < CLM_LOG_NTAB; i += blockDim.x)
-        tab[i] = make_double2(c_logtab[2 * i], c_logtab[2 * i + 1]);
+    for (int i = threadIdx.x; i < CLM_SC_N * SC_COPIES; i += blockDim.x) {
+        const int e = i / SC_COPIES;
+        sctab[i] = make_double2(c_sctab[2 * e], c_sctab[2 * e + 1]);
+    }
+    for (int i = threadIdx.x; i < CLM_LOG_NTAB * LOG_COPIES; i += blockDim.x) {
+        const int e = i / LOG_COPIES;
+        tab[i] = make_double2(c_logtab[2 * e], c_logtab[2 * e + 1]);
+    }
 }
 
 struct KArgs {
@@ -137,6 +152,9 @@ enum : int32_t { FK_NONE = 0, FK_READOUT = 1, FK_POLISHED = 2, FK_FACET = 3 };
 #ifndef CL_FILL_BLOCKS
 #define CL_FILL_BLOCKS 2
 #endif
+#ifndef CL_NEED_BY_STATE
+#define CL_NEED_BY_STATE 0
+#endif
 #ifndef CL_MIN_CTAS_PER_SM
 #define CL_MIN_CTAS_PER_SM 4
 #endif
@@ -170,6 +188,8 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
 
     const int lane = tid & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
+    const double2* my_tab = s_tab + (lane % LOG_COPIES);
+    const double2* my_sctab = s_sctab + (lane % SC_COPIES);
     const bool uni_possible = P.air_gap && P.sigma_alpha > 0.0f;
     const float inf = __int_as_float(0x7f800000);
 
@@ -244,7 +264,13 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
 
         // ---- top up the uniform ring: one Philox call site for the warp ----
         {
+#if CL_NEED_BY_STATE
+            // the most uniforms this lane's state can consume in one iteration
+            const int need = st == S_MOVE ? DRAWS_PER_ITER : (st == S_UNI ? 5 : (st == S_LAMB ? 2 : 3));
+            const bool want = st != S_IDLE && rng.cnt < need;
+#else
             const bool want = st != S_IDLE && rng.cnt < DRAWS_PER_ITER;
+#endif
             if (__any_sync(FULL, want)) {
 #if CL_FILL_JOIN
                 // every lane with room tops up at this convergent point, so
@@ -292,11 +318,11 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
         // so their Float64 dependency chains interleave (lanes that need none of
         // them get the harmless argument 1).
         float L0, L1, L2, s0, c0, s1, c1;
-        L0 = cl_logf_u(a0, s_tab);
-        L1 = cl_logf_u(a1, s_tab);
-        L2 = cl_logf_u(a2, s_tab);
-        cl_sincosf_core(p0, s_sctab, &s0, &c0);
-        cl_sincosf_core(p1, s_sctab, &s1, &c1);
+        L0 = cl_logf_u<LOG_COPIES>(a0, my_tab);
+        L1 = cl_logf_u<LOG_COPIES>(a1, my_tab);
+        L2 = cl_logf_u<LOG_COPIES>(a2, my_tab);
+        cl_sincosf_core<SC_COPIES>(p0, my_sctab, &s0, &c0);
+        cl_sincosf_core<SC_COPIES>(p1, my_sctab, &s1, &c1);
         (void)nl0; (void)nl1; (void)nl2; (void)ns0; (void)ns1;
 
         // ---- post, part 1 ----
@@ -388,7 +414,7 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
         // ---- facet tilt sin/cos, once per warp ----
         float sa = 0.f, ca = 1.f;
         if (__any_sync(FULL, facet)) {
-            cl_sincosf_core(facet ? alpha : 1.0f, s_sctab, &sa, &ca);
+            cl_sincosf_core<SC_COPIES>(facet ? alpha : 1.0f, my_sctab, &sa, &ca);
         }
 
         // UNIFIED try, second half (src/optics.jl:57-66): the facet normal
@@ -630,10 +656,10 @@ __global__ void debug_math_kernel(int fn, const float* in, float* out, int64_t n
         const float x = in[i];
         float r;
         if (fn == 0) {
-            r = cl_logf(x, s_tab);
+            r = cl_logf<LOG_COPIES>(x, s_tab + (threadIdx.x % LOG_COPIES));
         } else {
             float sv, cv;
-            cl_sincosf(x, s_sctab, &sv, &cv);
+            cl_sincosf<SC_COPIES>(x, s_sctab + (threadIdx.x % SC_COPIES), &sv, &cv);
             r = fn == 1 ? sv : cv;
         }
         out[i] = r;
