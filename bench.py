@@ -7,6 +7,14 @@ Workload (one "step" = one pass over it):
            point = 51.2M photons, per-point 8x8 count and first-hit maps.
   point1m  CsI(Tl) + Teflon 48x48x37.2 mm, 1,000,000 photons from the centre,
            8x8x81 count histogram and 8x8 first-hit map.
+  events_csitl          50,000 511 keV gammas on CsI(Tl) + Teflon: events/s.
+  events_bgo_surrogate  500,000 511 keV gammas on BGO + ESR through the
+           learned surrogate with Monte Carlo fallback, against the plain
+           Monte Carlo of the same events: events/s.
+
+The default run adds two secondary objects to its line: the 511 keV events/s
+of the event pipeline (a 10,000-event sample of events_csitl, --events) and
+events_bgo_surrogate (--surrogate-events).
 
 Arms:
   --impl cuda       (default) the sm_100a library; `value` = photons/s with
@@ -45,7 +53,7 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per launch of the transport kernel from ncu
 # (profiles/transport_kernel_*.md); independent of the photon count: the only
 # DRAM traffic is the sources, offsets and output maps.
-TRAFFIC_BYTES = {"scan256": 218_624, "point1m": 82_944}
+TRAFFIC_BYTES = {"scan256": 244_224, "point1m": 82_944}
 
 
 def events_workload(n_events: int = 50_000):
@@ -563,6 +571,16 @@ def run_cuda_arm(args, W, rank, world, local_rank):
                           "value": r["value"], "e2e": r["e2e"], "unit": "events/s",
                           "photons_per_event": r["photons"] / E["n_events"],
                           "photon_steps_per_s": r["photon_steps"] / r["dev_s"]}
+    if world == 1 and args.surrogate_events > 0 and os.path.exists(SURROGATE_BGO):
+        # secondary metric: config 5, surrogate + Monte Carlo fallback vs the plain Monte Carlo
+        E = surrogate_events_workload(args.surrogate_events)
+        r = run_surrogate_events_bench(eng, E, min(args.steps, 3), args.warmup, dev, stream)
+        line["surrogate_events"] = {
+            "metric": "511keV events/s", "workload": E["desc"], "unit": "events/s",
+            "value": r["value"], "e2e": r["e2e"], "plain_mc": r["mc_value"],
+            "speedup_vs_plain_mc": r["value"] / r["mc_value"],
+            "photopeak_shift": r["photopeak_shift"], "maps_vs_mc": r["maps"],
+            "fallback_sites": r["stats"]["fallback_sites"], "sites": r["stats"]["sites"]}
     print(json.dumps(line), flush=True)
     eng.close()
 
@@ -698,6 +716,9 @@ def main():
     ap.add_argument("--events", type=int, default=10_000,
                     help="events in the secondary events/s measurement of the default run "
                          "(0 = skip)")
+    ap.add_argument("--surrogate-events", type=int, default=500_000,
+                    help="events in the secondary surrogate-vs-Monte-Carlo measurement of the "
+                         "default run (0 = skip)")
     ap.add_argument("--n-events", type=int, default=0,
                     help="events of --workload events_csitl (default 50000) or "
                          "events_bgo_surrogate (default 500000)")
