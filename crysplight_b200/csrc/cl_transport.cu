@@ -90,6 +90,7 @@ struct KArgs {
     unsigned long long* steps;
     unsigned int* done;
     unsigned int* err;
+    const float* logtab;  // log of every uniform (k+1)*2^-24 at [k], or NULL: compute
 };
 
 __device__ __forceinline__ int time_bin0(float t, const Physics& P)
@@ -154,6 +155,9 @@ enum : int32_t { FK_NONE = 0, FK_READOUT = 1, FK_POLISHED = 2, FK_FACET = 3 };
 #endif
 #ifndef CL_NEED_BY_STATE
 #define CL_NEED_BY_STATE 0
+#endif
+#ifndef CL_USE_LOGTAB
+#define CL_USE_LOGTAB 1
 #endif
 #ifndef CL_MIN_CTAS_PER_SM
 #define CL_MIN_CTAS_PER_SM 4
@@ -318,9 +322,18 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
         // so their Float64 dependency chains interleave (lanes that need none of
         // them get the harmless argument 1).
         float L0, L1, L2, s0, c0, s1, c1;
-        L0 = cl_logf_u<LOG_COPIES>(a0, my_tab);
-        L1 = cl_logf_u<LOG_COPIES>(a1, my_tab);
-        L2 = cl_logf_u<LOG_COPIES>(a2, my_tab);
+        if (A.logtab) {
+            // the logs' arguments are uniforms (k+1)*2^-24: look them up
+            // (issued before the sincos work so the loads overlap it)
+            // (the index is clamped into the table whatever the argument)
+            L0 = __ldg(A.logtab + min((uint32_t)(a0 * 16777216.0f) - 1u, 0xFFFFFFu));
+            L1 = __ldg(A.logtab + min((uint32_t)(a1 * 16777216.0f) - 1u, 0xFFFFFFu));
+            L2 = __ldg(A.logtab + min((uint32_t)(a2 * 16777216.0f) - 1u, 0xFFFFFFu));
+        } else {
+            L0 = cl_logf_u<LOG_COPIES>(a0, my_tab);
+            L1 = cl_logf_u<LOG_COPIES>(a1, my_tab);
+            L2 = cl_logf_u<LOG_COPIES>(a2, my_tab);
+        }
         cl_sincosf_core<SC_COPIES>(p0, my_sctab, &s0, &c0);
         cl_sincosf_core<SC_COPIES>(p1, my_sctab, &s1, &c1);
         (void)nl0; (void)nl1; (void)nl2; (void)ns0; (void)ns1;
@@ -623,6 +636,19 @@ __global__ void init_kernel(uint32_t* counts, int64_t n_counts, uint32_t* keys, 
     if (i0 == 0) { *queue = 0ull; *steps = 0ull; *done = 0u; *err = 0u; }
 }
 
+// The log table of the uniforms: t[k] = cl_logf_u((k+1) * 2^-24), the same
+// function and rounding as the computed path, for k < 2^24.
+__global__ void logtab_fill(float* t)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2 *s_tab, *s_sctab;
+    load_tables(smem, s_tab, s_sctab);
+    __syncthreads();
+    const double2* my_tab = s_tab + (threadIdx.x % LOG_COPIES);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < (1u << 24); k += gridDim.x * blockDim.x)
+        t[k] = cl_logf_u<LOG_COPIES>(u32_to_randu(k << 8), my_tab);
+}
+
 // Segment mode: decode tmin keys in place and sum npe per segment.
 __global__ void finalize_segments(const uint32_t* maps, uint32_t* keys, int32_t* npe,
                                   int64_t n_seg, int32_t cells)
@@ -707,6 +733,7 @@ struct cl_handle {
     int device = 0;
     int num_sms = 0;
     cudaStream_t stream = nullptr;
+    DevBuf logtab;                 // 2^24 floats, or empty: the kernels compute the logs
     char err[512] = {0};
     DevBuf src, out, rec, scratch, dbg;
     int ctas_per_sm = 0;
@@ -822,6 +849,22 @@ int cl_create(cl_handle** out, int device)
         delete h;
         return CL_ERR_OOM;
     }
+#if CL_USE_LOGTAB
+    // 64 MB table of the logs of all 2^24 uniforms; without it (allocation
+    // failure) the kernels evaluate the same function in place
+    if (cudaMalloc(&h->logtab.p, sizeof(float) << 24) == cudaSuccess) {
+        h->logtab.cap = sizeof(float) << 24;
+        logtab_fill<<<h->num_sms * 4, 256, LOGTAB_BYTES, h->stream>>>((float*)h->logtab.p);
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(h->logtab.p);
+            h->logtab = DevBuf();
+        }
+    } else {
+        cudaGetLastError();
+        h->logtab = DevBuf();
+    }
+#endif
     *out = h;
     return CL_OK;
 }
@@ -831,7 +874,7 @@ void cl_destroy(cl_handle* h)
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    DevBuf* bufs[] = {&h->src, &h->out, &h->rec, &h->scratch, &h->dbg};
+    DevBuf* bufs[] = {&h->src, &h->out, &h->rec, &h->scratch, &h->dbg, &h->logtab};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -977,6 +1020,7 @@ static int enqueue_point(cl_handle* h, const Physics& P, const float* px, const 
     const bool want_rec = rec && (rec->status || rec->idx || rec->t || rec->bounces);
     if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
     a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
+    a.logtab = (const float*)h->logtab.p;
     const size_t tile_bytes = ((size_t)n_counts + cells) * sizeof(uint32_t);
     const size_t base_bytes = LOGTAB_BYTES + (size_t)RING_LEN * RING_STRIDE * sizeof(float);
     const bool tile = base_bytes + tile_bytes <= (size_t)std::min(h->max_smem_optin, 160 * 1024);
@@ -1017,6 +1061,7 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
         const bool want_rec = rec && (rec->status || rec->idx || rec->t || rec->bounces);
         if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
         a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
+        a.logtab = (const float*)h->logtab.p;
         const size_t smem = LOGTAB_BYTES + (size_t)RING_LEN * RING_STRIDE * sizeof(float);
         a.tsum = tsum; a.tsum2 = tsum2;
         const int rc = moments ? launch_transport<2, false, false>(h, a, smem, st)
