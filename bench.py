@@ -71,47 +71,36 @@ def events_workload(n_events: int = 50_000):
 
 
 def run_events_bench(eng, E, steps: int, warmup: int, dev, stream, pid_base: int = 0):
-    """events/s: transport of all events' photons with the deposits in HBM
-    (value), and the whole public pipeline run_events (e2e)."""
+    """events/s: the transport of all events' photons with the deposits in HBM
+    (value: one CUDA-graph replay of init + transport + finalize per step, at
+    the launch shape the autotuner picked), and the whole public pipeline
+    run_events (e2e)."""
     import torch
+    from crysplight_b200.batching import DeviceEvents, autotune
     from crysplight_b200.events import gamma_stage, run_events
     g = gamma_stage(E["mat"], E["box"], n_events=E["n_events"], seed=E["seed"],
                     yield_per_mev=E["yield_"])
     nd = g.dep_photons.size
-    off = np.zeros(nd + 1, np.int64)
-    np.cumsum(g.dep_photons, out=off[1:])
-    d = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in
-         dict(x=g.dep_xyz[:, 0], y=g.dep_xyz[:, 1], z=g.dep_xyz[:, 2], t=g.dep_t, off=off,
-              seg=g.dep_event).items()}
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     n_seg = E["n_events"]
-    maps = torch.empty(64 * n_seg, dtype=torch.int32, device=dev)
-    tmin = torch.empty(64 * n_seg, dtype=torch.float32, device=dev)
-    npe = torch.empty(n_seg, dtype=torch.int32, device=dev)
-    ctr = torch.empty(9, dtype=torch.int64, device=dev)
-    sptr = stream.cuda_stream
-
-    def step():
-        eng.run_segments_device(E["box"], E["op"], E["ro"], E["tb"], sx=d["x"].data_ptr(),
-                                sy=d["y"].data_ptr(), sz=d["z"].data_ptr(), st=d["t"].data_ptr(),
-                                src_offsets=d["off"].data_ptr(), src_segment=d["seg"].data_ptr(),
-                                n_src=nd, n_segments=n_seg, n_photons=int(off[-1]),
-                                seed=E["seed"], pid_offset=pid_base, tau_ns=E["tau"],
-                                maps=maps.data_ptr(), tmin=tmin.data_ptr(), npe=npe.data_ptr(),
-                                counters=ctr.data_ptr(), stream=sptr)
+    ev = DeviceEvents(eng, E["box"], E["op"], E["ro"], E["tb"], xyz=T(g.dep_xyz), t0=T(g.dep_t),
+                      photons=T(g.dep_photons), segment=T(g.dep_event), n_segments=n_seg,
+                      seed=E["seed"], tau_ns=E["tau"], pid_offset=pid_base)
+    best, tune_times = autotune(eng, ev.step, stream=stream, repeats=2)
+    ev.capture()
     for _ in range(warmup):
-        step()
-    eng.sync(sptr)
+        ev.replay()
+    ev.sync(stream)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(steps)]
-    for a, b in ev:
+    marks = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+             for _ in range(steps)]
+    for a, b in marks:
         flush.zero_()
         a.record(stream)
-        step()
+        ev.replay()
         b.record(stream)
-    eng.sync(sptr)
-    torch.cuda.synchronize(dev)
-    dev_s = sum(a.elapsed_time(b) for a, b in ev) * 1e-3 / steps
+    ev.sync(stream)
+    dev_s = sum(a.elapsed_time(b) for a, b in marks) * 1e-3 / steps
     photon_steps = eng.last_steps
     run_events(E["box"], E["op"], E["ro"], E["tb"], E["mat"], E["yield_"],
                n_events=E["n_events"], seed=E["seed"], tau_ns=E["tau"], engine=eng)
@@ -120,9 +109,14 @@ def run_events_bench(eng, E, steps: int, warmup: int, dev, stream, pid_base: int
         run_events(E["box"], E["op"], E["ro"], E["tb"], E["mat"], E["yield_"],
                    n_events=E["n_events"], seed=E["seed"], tau_ns=E["tau"], engine=eng)
     e2e_s = (time.perf_counter() - t0) / steps
+    eng.set_launch(0, 0, 0)
     return dict(value=E["n_events"] / dev_s, e2e=E["n_events"] / e2e_s, dev_s=dev_s,
-                e2e_s=e2e_s, photons=int(off[-1]), photon_steps=photon_steps, deposits=nd,
-                h2d=int(3 * 4 * nd + 4 * nd + 8 * (nd + 1) + 4 * nd),
+                e2e_s=e2e_s, photons=ev.n_photons, photon_steps=photon_steps, deposits=nd,
+                launch={"ctas_per_sm": best.ctas_per_sm, "threads_per_cta": best.threads_per_cta,
+                        "warp_chunk": best.warp_chunk},
+                tune_ms={f"{k.threads_per_cta}x{k.ctas_per_sm}/{k.warp_chunk}": round(v * 1e3, 3)
+                         for k, v in tune_times.items()},
+                h2d=int(3 * 4 * nd + 4 * nd + 8 * nd + 4 * nd),
                 d2h=int(2 * 4 * 64 * n_seg + 4 * n_seg + 72 + 12))
 
 
@@ -570,7 +564,8 @@ def run_cuda_arm(args, W, rank, world, local_rank):
         line["events"] = {"metric": "511keV events/s", "workload": E["desc"],
                           "value": r["value"], "e2e": r["e2e"], "unit": "events/s",
                           "photons_per_event": r["photons"] / E["n_events"],
-                          "photon_steps_per_s": r["photon_steps"] / r["dev_s"]}
+                          "photon_steps_per_s": r["photon_steps"] / r["dev_s"],
+                          "launch": r["launch"], "cuda_graph": True}
     if world == 1 and args.surrogate_events > 0 and os.path.exists(SURROGATE_BGO):
         # secondary metric: config 5, surrogate + Monte Carlo fallback vs the plain Monte Carlo
         E = surrogate_events_workload(args.surrogate_events)
@@ -629,7 +624,8 @@ def run_events_arm(args, rank, world, local_rank):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": E["name"], "desc": E["desc"],
                            "photons_per_step": r["photons"], "deposits": r["deposits"],
-                           "l2": "flushed between timed steps (256 MiB memset)"},
+                           "l2": "flushed between timed steps (256 MiB memset)",
+                           "cuda_graph": True, "launch": r["launch"], "autotune_ms": r["tune_ms"]},
                 "e2e": {"value": world * E["n_events"] / e2e_s, "unit": "events/s",
                         "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
                 "gpu_launches": 3 * args.steps,
