@@ -159,6 +159,15 @@ enum : int32_t { FK_NONE = 0, FK_READOUT = 1, FK_POLISHED = 2, FK_FACET = 3 };
 #ifndef CL_USE_LOGTAB
 #define CL_USE_LOGTAB 1
 #endif
+#ifndef CL_DEFAULT_WARP_CHUNK
+#define CL_DEFAULT_WARP_CHUNK 0
+#endif
+#ifndef CL_CHUNKS_PER_WARP
+#define CL_CHUNKS_PER_WARP 16
+#endif
+#ifndef CL_MAX_WARP_CHUNK
+#define CL_MAX_WARP_CHUNK 256
+#endif
 #ifndef CL_MIN_CTAS_PER_SM
 #define CL_MIN_CTAS_PER_SM 4
 #endif
@@ -738,7 +747,7 @@ struct cl_handle {
     DevBuf src, out, rec, scratch, dbg;
     int ctas_per_sm = 0;
     int threads = 256;
-    int warp_chunk = 64;
+    int warp_chunk = CL_DEFAULT_WARP_CHUNK;   // 0: automatic per launch
     int64_t last_steps = 0;
     int max_smem_optin = 0;
 };
@@ -894,7 +903,7 @@ int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta, int warp_c
         return set_err(h, CL_ERR_ARG, "warp_chunk must be in [32, 2^20]");
     h->ctas_per_sm = ctas_per_sm;
     h->threads = threads_per_cta ? threads_per_cta : 256;
-    h->warp_chunk = warp_chunk ? warp_chunk : 64;
+    h->warp_chunk = warp_chunk ? warp_chunk : CL_DEFAULT_WARP_CHUNK;
     return CL_OK;
 }
 
@@ -984,11 +993,21 @@ static int launch_transport(cl_handle* h, const KArgs& a, size_t smem, cudaStrea
     if (per_sm < 1) return set_err(h, CL_ERR_ARG, "transport kernel does not fit on an SM (shared tile too large)");
     if (h->ctas_per_sm > 0 && h->ctas_per_sm < per_sm) per_sm = h->ctas_per_sm;
     int64_t grid = (int64_t)h->num_sms * per_sm;
+    KArgs b = a;
+    if (b.warp_chunk <= 0) {
+        // automatic: the largest chunk (fewest queue atomics) that still gives
+        // every resident warp about CL_CHUNKS_PER_WARP chunks, so the end of
+        // the queue stays balanced; between 32 and CL_MAX_WARP_CHUNK photons
+        const int64_t warps = grid * (h->threads / 32);
+        int64_t c = a.n / (warps * CL_CHUNKS_PER_WARP);
+        c = c < 32 ? 32 : (c > CL_MAX_WARP_CHUNK ? CL_MAX_WARP_CHUNK : c);
+        b.warp_chunk = (int32_t)(c & ~(int64_t)31);
+    }
     // no more CTAs than warps' worth of first chunks
-    const int64_t warps_needed = (a.n + a.warp_chunk - 1) / a.warp_chunk;
+    const int64_t warps_needed = (b.n + b.warp_chunk - 1) / b.warp_chunk;
     const int64_t ctas_needed = (warps_needed + (h->threads / 32) - 1) / (h->threads / 32);
     if (grid > ctas_needed) grid = ctas_needed > 0 ? ctas_needed : 1;
-    kern<<<(unsigned)grid, h->threads, smem, st>>>(a);
+    kern<<<(unsigned)grid, h->threads, smem, st>>>(b);
     CK(h, cudaGetLastError(), "transport kernel launch");
     return CL_OK;
 }
