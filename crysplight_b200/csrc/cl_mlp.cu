@@ -72,10 +72,13 @@ struct GemmArgs {
     unsigned int* err;
 };
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU and its derivative with the fast exponential and division (results
+// are rounded to BF16 afterwards; for z -> -inf, __fdividef by an infinite
+// denominator returns 0)
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z)
 {
-    const float s = 1.0f / (1.0f + __expf(-z));
+    const float s = __fdividef(1.0f, 1.0f + __expf(-z));
     return s * (1.0f + z * (1.0f - s));
 }
 
