@@ -32,9 +32,12 @@ using bf16 = __nv_bfloat16;
 
 constexpr int TILE_M = 128;     // rows per CTA tile (TMEM lanes)
 constexpr int TILE_K = 64;      // K elements per pipeline stage (one 128-byte swizzle row)
-constexpr int STAGES = 4;       // TMA -> MMA pipeline depth
-constexpr int EPI_WARPS = 4;    // warps 0-3: epilogue (TMEM lane quadrants 0-3)
-constexpr int GEMM_THREADS = 192;   // + warp 4: TMA producer, warp 5: MMA issuer / TMEM owner
+constexpr int STAGES = 3;       // TMA -> MMA pipeline depth
+constexpr int EPI_WARPS = 8;    // warps 0-7: epilogue; warp w drains TMEM lane quadrant w % 4,
+                                // 32-column chunks c with c % 2 == w / 4
+constexpr int PRODUCER_WARP = EPI_WARPS;        // TMA producer
+constexpr int MMA_WARP = EPI_WARPS + 1;         // MMA issuer / TMEM owner
+constexpr int GEMM_THREADS = 32 * (EPI_WARPS + 2);
 constexpr uint32_t TMEM_COLS = 512; // two 256-column FP32 accumulators
 constexpr uint32_t WAIT_BUDGET = 1u << 22;   // polls before a wait gives up
 constexpr int RED_STRIDE = 33;
@@ -113,9 +116,11 @@ __device__ __forceinline__ void store_row_bf16(bf16* dst, const bf16* h)
     for (int i = 0; i < 4; ++i) d[i] = reinterpret_cast<const uint4*>(h)[i];
 }
 
-// Epilogue of one 128 x N tile: warp w owns rows row0 + 32w + lane.
+// Epilogue of one 128 x N tile: the warp owns rows row0 + 32 (w % 4) + lane and
+// the 32-column chunks c0 = 32 (half + 2 k).
 template <int EPI>
-__device__ __forceinline__ void epilogue(const GemmArgs& G, uint32_t tbase, int row, float* red, int lane)
+__device__ __forceinline__ void epilogue(const GemmArgs& G, uint32_t tbase, int row, float* red, int lane,
+                                         int half)
 {
     const int N = G.N;
     float sq = 0.0f;
@@ -126,7 +131,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, uint32_t tbase, int 
         xs[lane * 3] = x0; xs[lane * 3 + 1] = x1; xs[lane * 3 + 2] = x2;
         __syncwarp();
     }
-    for (int c0 = 0; c0 < N; c0 += 32) {
+    for (int c0 = 32 * half; c0 < N; c0 += 64) {
         float v[32];
         umma::tmem_ld32(tbase + (uint32_t)c0, v);
         if (EPI == EPI_F32 || EPI == EPI_BIAS_F32 || EPI == EPI_PARTIAL) {
@@ -240,14 +245,14 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         for (int a = 0; a < 2; ++a) { umma::mbar_init(&acc_full[a], 1); umma::mbar_init(&acc_empty[a], EPI_WARPS); }
         abort_flag = 0;
     }
-    if (warp == 5) umma::tmem_alloc(&tmem_slot, TMEM_COLS);
-    if (warp == 4 && lane == 0) { umma::prefetch_tmap(&tmA); umma::prefetch_tmap(&tmB); }
+    if (warp == MMA_WARP) umma::tmem_alloc(&tmem_slot, TMEM_COLS);
+    if (warp == PRODUCER_WARP && lane == 0) { umma::prefetch_tmap(&tmA); umma::prefetch_tmap(&tmB); }
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = tmem_slot;
 
-    if (warp == 4) {
+    if (warp == PRODUCER_WARP) {
         if (lane == 0) {
             uint32_t it = 0;
             bool ok = true;
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             for (uint32_t j = it > (uint32_t)STAGES ? it - STAGES : 0u; j < it; ++j)
                 umma::mbar_wait(&full[j % STAGES], (j / STAGES) & 1u, WAIT_BUDGET);
         }
-    } else if (warp == 5) {
+    } else if (warp == MMA_WARP) {
         if (lane == 0) {
             const uint32_t idesc = umma::make_idesc_bf16(TILE_M, N);
             uint32_t it = 0, j = 0;
@@ -311,15 +316,16 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                 break;
             }
             umma::fence_after_sync();
-            const int row = tile * TILE_M + 32 * warp + lane;
-            epilogue<EPI>(G, tmem + a * 256u + ((uint32_t)(32 * warp) << 16), row, red, lane);
+            const int quad = warp & 3;
+            const int row = tile * TILE_M + 32 * quad + lane;
+            epilogue<EPI>(G, tmem + a * 256u + ((uint32_t)(32 * quad) << 16), row, red, lane, warp >> 2);
             umma::fence_before_sync();
             __syncwarp();
             if (lane == 0) umma::mbar_arrive(&acc_empty[a]);
         }
     }
     __syncthreads();
-    if (warp == 5) {
+    if (warp == MMA_WARP) {
         umma::fence_after_sync();
         umma::tmem_dealloc(tmem, TMEM_COLS);
     }
