@@ -8,6 +8,10 @@
 // SiLU', the loss and its gradient, bias-gradient column sums, the layer-1
 // gradients, BF16 casts, transposed copies, split-K partials).  The 3-wide
 // input layer, the split-K reduction and Adam run on the CUDA cores.
+// The epilogues are element-wise work over the 128 x N accumulator of every
+// tile; they are spread over sixteen warps (four per TMEM lane quadrant, each
+// taking every fourth 32-column chunk) so that draining a tile keeps pace
+// with the tensor cores filling the other accumulator.
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -33,8 +37,11 @@ using bf16 = __nv_bfloat16;
 constexpr int TILE_M = 128;     // rows per CTA tile (TMEM lanes)
 constexpr int TILE_K = 64;      // K elements per pipeline stage (one 128-byte swizzle row)
 constexpr int STAGES = 3;       // TMA -> MMA pipeline depth
-constexpr int EPI_WARPS = 8;    // warps 0-7: epilogue; warp w drains TMEM lane quadrant w % 4,
-                                // 32-column chunks c with c % 2 == w / 4
+#ifndef CL_MLP_EPI_WARPS
+#define CL_MLP_EPI_WARPS 16
+#endif
+constexpr int EPI_WARPS = CL_MLP_EPI_WARPS;   // epilogue warps: warp w drains TMEM lane quadrant w % 4,
+                                             // 32-column chunks c with c % (EPI_WARPS/4) == w / 4
 constexpr int PRODUCER_WARP = EPI_WARPS;        // TMA producer
 constexpr int MMA_WARP = EPI_WARPS + 1;         // MMA issuer / TMEM owner
 constexpr int GEMM_THREADS = 32 * (EPI_WARPS + 2);
@@ -131,7 +138,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, uint32_t tbase, int 
         xs[lane * 3] = x0; xs[lane * 3 + 1] = x1; xs[lane * 3 + 2] = x2;
         __syncwarp();
     }
-    for (int c0 = 32 * half; c0 < N; c0 += 64) {
+    for (int c0 = 32 * half; c0 < N; c0 += 32 * (EPI_WARPS / 4)) {
         float v[32];
         umma::tmem_ld32(tbase + (uint32_t)c0, v);
         if (EPI == EPI_F32 || EPI == EPI_BIAS_F32 || EPI == EPI_PARTIAL) {
