@@ -12,9 +12,10 @@ Workload (one "step" = one pass over it):
            learned surrogate with Monte Carlo fallback, against the plain
            Monte Carlo of the same events: events/s.
 
-The default run adds two secondary objects to its line: the 511 keV events/s
-of the event pipeline (a 10,000-event sample of events_csitl, --events) and
-events_bgo_surrogate (--surrogate-events).
+The default run adds secondary objects to its line: the 511 keV events/s of
+the event pipeline (a 10,000-event sample of events_csitl, --events), the
+surrogate MLP's training throughput on the tensor cores
+(--surrogate-training), and events_bgo_surrogate (--surrogate-events).
 
 Arms:
   --impl cuda       (default) the sm_100a library; `value` = photons/s with
@@ -118,6 +119,32 @@ def run_events_bench(eng, E, steps: int, warmup: int, dev, stream, pid_base: int
                          for k, v in tune_times.items()},
                 h2d=int(3 * 4 * nd + 4 * nd + 8 * nd + 4 * nd),
                 d2h=int(2 * 4 * 64 * n_seg + 4 * n_seg + 72 + 12))
+
+
+def surrogate_training_bench(dev, steps: int = 200, warmup: int = 20) -> dict:
+    """Adam steps of the surrogate MLP (3->256->256->256->192, batch 65,536) on
+    the tcgen05 kernels, synthetic training data: ms per step and TFLOP/s
+    against the measured dense BF16 peak (sustained: a long loop)."""
+    import torch
+    from crysplight_b200.surrogate import MLP
+    n = 55_296
+    g = torch.Generator(device=dev).manual_seed(3)
+    x = torch.rand(n, 3, device=dev, generator=g) * 2 - 1
+    t = torch.randn(n, 192, device=dev, generator=g)
+    m = MLP(dev.index or 0, max_batch=65536, seed=1)
+    m.set_data(x, t)
+    m.train(warmup, batch=65536)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    m.train(steps, batch=65536)
+    torch.cuda.synchronize(dev)
+    dt = (time.perf_counter() - t0) / steps
+    m.close()
+    flop = 65536 * 2 * 3 * (3 * 256 + 2 * 256 * 256 + 256 * 192)      # forward + 2 x backward
+    peak = measured_peaks().get("bf16_tflops_sustained", 1400.0)
+    return {"metric": "surrogate training steps/s", "batch": 65536, "ms_per_step": dt * 1e3,
+            "tflops": flop / dt / 1e12, "peak_tflops": peak, "frac": flop / dt / 1e12 / peak,
+            "note": "one cl_mlp_train call of all steps (host time around a synchronised loop)"}
 
 
 SURROGATE_BGO = os.path.join(ROOT, "crysplight_b200", "surrogates", "bgo_esr.npz")
@@ -566,6 +593,8 @@ def run_cuda_arm(args, W, rank, world, local_rank):
                           "photons_per_event": r["photons"] / E["n_events"],
                           "photon_steps_per_s": r["photon_steps"] / r["dev_s"],
                           "launch": r["launch"], "cuda_graph": True}
+    if world == 1 and args.surrogate_training:
+        line["surrogate_training"] = surrogate_training_bench(dev)
     if world == 1 and args.surrogate_events > 0 and os.path.exists(SURROGATE_BGO):
         # secondary metric: config 5, surrogate + Monte Carlo fallback vs the plain Monte Carlo
         E = surrogate_events_workload(args.surrogate_events)
@@ -712,6 +741,8 @@ def main():
     ap.add_argument("--events", type=int, default=10_000,
                     help="events in the secondary events/s measurement of the default run "
                          "(0 = skip)")
+    ap.add_argument("--surrogate-training", type=int, default=1,
+                    help="add the surrogate MLP's training throughput to the default line (0 = skip)")
     ap.add_argument("--surrogate-events", type=int, default=500_000,
                     help="events in the secondary surrogate-vs-Monte-Carlo measurement of the "
                          "default run (0 = skip)")

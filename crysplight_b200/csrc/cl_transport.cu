@@ -186,7 +186,6 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
 
     const Physics& P = A.P;
     const int tid = threadIdx.x;
-    const int stride = blockDim.x;
     if (TILE) {
         const int nt = A.cells * A.bins_total;
         for (int i = tid; i < nt; i += blockDim.x) s_counts[i] = 0u;
