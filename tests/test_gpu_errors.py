@@ -1,0 +1,70 @@
+"""Argument errors of the device entry points come back as CL_ERR_ARG with a
+message and leave the handle usable (the reference raises exceptions,
+src/config.jl:23,59); nothing is launched for a rejected call."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from cases import BOX_BGO, GRID, OP_C2, TB80
+
+pytestmark = pytest.mark.gpu
+
+
+def test_events_surrogate_rejects_bad_arguments(engine):
+    from crysplight_b200 import _lib
+    from crysplight_b200.params import Readout
+    lib = _lib.load()
+    P = C.c_void_p
+    ro = Readout(GRID)
+
+    def call(**over):
+        a = dict(n_src=0, n_photons=0, n_sites=0, n_segments=1, maps=1, tmin=1, npe=1, ctr=1, sx=None)
+        a.update(over)
+        return lib.cl_run_events_surrogate_device(
+            engine.handle, C.byref(BOX_BGO), C.byref(OP_C2), C.byref(ro), C.byref(TB80),
+            P(a["sx"]) if a["sx"] else None, None, None, None, None, None, a["n_src"], a["n_photons"],
+            1, 0, 1768.0, 100000, None, None, None, None, None, None, None, a["n_sites"], 2,
+            a["n_segments"], P(a["maps"]), P(a["tmin"]), P(a["npe"]), P(a["ctr"]), None, None)
+    assert call(n_segments=0) == _lib.CL_ERR_ARG
+    assert b"n_segments" in lib.cl_last_error(engine.handle)
+    assert call(n_photons=5) == _lib.CL_ERR_ARG                     # photons without sources
+    assert call(n_src=3) == _lib.CL_ERR_ARG                         # null source arrays
+    assert call(n_sites=4) == _lib.CL_ERR_ARG                       # null site arrays
+    assert call(maps=0) == _lib.CL_ERR_ARG
+    # the handle still works
+    res = engine.run_segments(BOX_BGO, OP_C2, GRID, TB80, sources=[(24.0, 24.0, 11.2)], photons_per_source=[500],
+                              segment_of_source=[0], n_segments=1, seed=1, tau_ns=0.0)
+    assert res.counters["ndet"] + res.counters["nabs_bulk"] + res.counters["nabs_wall"] + \
+        res.counters["nabs_sipm"] + res.counters["ncap"] == 500
+
+
+def test_combine_rejects_bad_arguments():
+    from crysplight_b200 import _lib
+    from crysplight_b200.params import Readout, SipmGrid
+    lib = _lib.load()
+    P = C.c_void_p
+    args = lambda ro, pde, members=5, n=10: (P(1), members, n, P(1), P(1), P(1), C.byref(BOX_BGO), C.byref(ro),
+                                             pde, 0.02, 1.0, P(1), P(1), P(1), P(1), P(1), None)
+    assert lib.cl_surrogate_combine(*args(Readout(SipmGrid(6.0, 4, 4)), 0.4)) == _lib.CL_ERR_ARG   # 16 cells
+    assert lib.cl_surrogate_combine(*args(Readout(GRID), 1.5)) == _lib.CL_ERR_ARG                   # PDE > 1
+    assert lib.cl_surrogate_combine(*args(Readout(GRID), 0.4, members=0)) == _lib.CL_ERR_ARG
+    assert lib.cl_surrogate_combine(*args(Readout(GRID), 0.4, n=0)) == _lib.CL_OK                    # nothing to do
+
+
+def test_mlp_rejects_bad_batches():
+    from crysplight_b200.surrogate import MLP
+    from crysplight_b200._lib import CudaTransportError
+    m = MLP(0, max_batch=1024, seed=0)
+    try:
+        import torch
+        x = torch.zeros(100, 3, device="cuda")
+        t = torch.zeros(100, 192, device="cuda")
+        m.set_data(x, t)
+        with pytest.raises(CudaTransportError):
+            m.train(1, batch=100)          # not a multiple of 128
+        with pytest.raises(CudaTransportError):
+            m.train(1, batch=2048)         # above max_batch
+        assert np.isfinite(m.train(2, batch=128))
+    finally:
+        m.close()
