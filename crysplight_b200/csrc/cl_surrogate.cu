@@ -336,6 +336,21 @@ __global__ void __launch_bounds__(CELLS * SITES_PER_CTA) surrogate_combine(const
     }
 }
 
+// Network inputs of the sites: x, y scaled to [-1, 1] and the depth through
+// w(t) = (1 - a) t + a (1 - sqrt(1 - t)), t = z / Lz clamped to [0, 1].
+__global__ void surrogate_inputs(const float* __restrict__ xyz, int64_t n, float L0, float L1, float L2,
+                                 float a, float* __restrict__ out)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        const float t = fminf(fmaxf(z / L2, 0.0f), 1.0f);
+        const float w = (1.0f - a) * t + a * (1.0f - sqrtf(1.0f - t));
+        out[3 * i] = 2.0f * x / L0 - 1.0f;
+        out[3 * i + 1] = 2.0f * y / L1 - 1.0f;
+        out[3 * i + 2] = 2.0f * w - 1.0f;
+    }
+}
+
 // Diagnostics: fn 0 = binomial(n = par[0], p = par[1]) -> int64,
 // fn 1 = emg_min(k = par[0], mu = par[1], sigma = par[2], tau = par[3]) -> double.
 __global__ void debug_sampler(int fn, double p0, double p1, double p2, double p3, int64_t n,
@@ -388,6 +403,19 @@ int cl_surrogate_combine(const float* d_raw, int32_t members, int64_t n_sites,
     const int64_t want = (n_sites + cl::sur::SITES_PER_CTA - 1) / cl::sur::SITES_PER_CTA;
     const unsigned grid = (unsigned)(want < 148 * 64 ? want : 148 * 64);
     cl::sur::surrogate_combine<<<grid, cl::sur::CELLS * cl::sur::SITES_PER_CTA, 0, (cudaStream_t)stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
+}
+
+int cl_surrogate_inputs(const float* d_xyz, int64_t n_sites, const cl_box* box, float z_warp, float* d_out,
+                        void* stream)
+{
+    if (!box || n_sites < 0 || !(z_warp >= 0.0f && z_warp <= 1.0f)) return CL_ERR_ARG;
+    if (n_sites == 0) return CL_OK;
+    if (!d_xyz || !d_out) return CL_ERR_ARG;
+    const int64_t want = (n_sites + 255) / 256;
+    const unsigned grid = (unsigned)(want < 148 * 32 ? want : 148 * 32);
+    cl::sur::surrogate_inputs<<<grid, 256, 0, (cudaStream_t)stream>>>(d_xyz, n_sites, box->L[0], box->L[1],
+                                                                      box->L[2], z_warp, d_out);
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
 }
 

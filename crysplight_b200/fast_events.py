@@ -7,7 +7,8 @@ transports every scintillation photon of every deposit.  Here each deposit
 resident on the GPU, evaluated by the library's tcgen05 forward kernels); the
 ensemble mean gives per SiPM the probability that one photon emitted at the
 site is detected there, and the transit-time mean and spread of the detected
-photons.  A site is sent to the Monte Carlo instead when the members disagree
+photons (the sites' inputs are scaled, and the depth warped, on the device by
+``cl_surrogate_inputs``).  A site is sent to the Monte Carlo instead when the members disagree
 (relative spread above ``spread_max``, default 2%), when it lies within
 ``wall_min_mm`` (default 1 mm) of a wrapped face, where the light response
 changes fastest, or when its probabilities do not form a valid split.
@@ -39,21 +40,6 @@ SPREAD_MAX = 0.02
 WALL_MIN_MM = 1.0
 
 
-def fold_input_scaling(params: np.ndarray, box_mm) -> np.ndarray:
-    """Parameters of the same network for inputs in mm: the training input
-    x_n = 2 x / L - 1 is folded into the first layer (W1 x_n + b1 =
-    (W1 diag(2/L)) x + (b1 - W1 1)), evaluated in float64."""
-    p = np.asarray(params, np.float64).copy()
-    L = np.asarray(box_mm, np.float64)
-    W1 = p[:256 * 3].reshape(256, 3)
-    b1 = p[256 * 3:256 * 4]
-    b1_new = b1 - W1.sum(1)
-    W1_new = W1 * (2.0 / L)[None, :]
-    p[:256 * 3] = W1_new.ravel()
-    p[256 * 3:256 * 4] = b1_new
-    return p.astype(np.float32)
-
-
 @dataclass
 class SiteLight:
     """Per-site outputs of the ensemble (CUDA tensors)."""
@@ -80,7 +66,7 @@ class SurrogateEvents:
         self.nets = []
         for p in surrogate.members:
             net = MLP(device, max_batch=max_batch, seed=0)
-            net.set_params(fold_input_scaling(p, surrogate.box_mm))
+            net.set_params(p)
             self.nets.append(net)
         self.y_mean = torch.from_numpy(np.ascontiguousarray(surrogate.y_mean, np.float32)).to(self.dev)
         self.y_std = torch.from_numpy(np.ascontiguousarray(surrogate.y_std, np.float32)).to(self.dev)
@@ -98,10 +84,17 @@ class SurrogateEvents:
         n = int(xyz.shape[0])
         K = len(self.nets)
         xyz = xyz.contiguous()
+        xin = torch.empty((n, 3), dtype=torch.float32, device=self.dev)
+        rc = self.lib.cl_surrogate_inputs(C.c_void_p(xyz.data_ptr()), n, C.byref(self.box),
+                                          float(self.sur.z_warp), C.c_void_p(xin.data_ptr()),
+                                          C.c_void_p(stream) if stream else None)
+        if rc != 0:
+            raise _lib.CudaTransportError(rc, "cl_surrogate_inputs failed")
+        torch.cuda.synchronize(self.dev)         # the networks run on their own streams
         raw = torch.empty((K, n, D_OUT), dtype=torch.float32, device=self.dev)
         for k, net in enumerate(self.nets):
             if n:
-                net.forward_into(xyz, raw[k])
+                net.forward_into(xin, raw[k])
         out = SiteLight(torch.empty((n, N_CELLS), dtype=torch.float32, device=self.dev),
                         torch.empty((n, N_CELLS), dtype=torch.float32, device=self.dev),
                         torch.empty((n, N_CELLS), dtype=torch.float32, device=self.dev),

@@ -142,12 +142,37 @@ class MLP:
 # ---------------------------------------------------------------------------
 # Training data: a point scan through the CUDA Monte Carlo
 # ---------------------------------------------------------------------------
-def grid_points(box: Box, shape=(48, 48, 24)) -> np.ndarray:
+def depth_warp(t, a: float):
+    """Warped depth w(t) = (1 - a) t + a (1 - sqrt(1 - t)) of t = z / Lz in
+    [0, 1] (the readout face at t = 1): monotonic, w(0) = 0, w(1) = 1, and
+    with a > 0 stretched near the readout face, where the light of a point
+    concentrates under one SiPM.  a = 0 is the identity."""
+    t = np.clip(np.asarray(t, np.float64), 0.0, 1.0)
+    return (1.0 - a) * t + a * (1.0 - np.sqrt(1.0 - t))
+
+
+def depth_unwarp(w, a: float):
+    """The t with depth_warp(t, a) = w (bisection; w in [0, 1])."""
+    w = np.asarray(w, np.float64)
+    lo, hi = np.zeros_like(w), np.ones_like(w)
+    for _ in range(60):
+        mid = 0.5 * (lo + hi)
+        below = depth_warp(mid, a) < w
+        lo = np.where(below, mid, lo)
+        hi = np.where(below, hi, mid)
+    return 0.5 * (lo + hi)
+
+
+def grid_points(box: Box, shape=(48, 48, 24), z_warp: float = 0.0) -> np.ndarray:
     """Cell centres of a regular nx x ny x nz grid over the crystal, (P, 3)
-    float32 in mm, x fastest."""
+    float32 in mm, x fastest; with ``z_warp`` the z levels are the cell
+    centres of a regular grid in the warped depth (denser towards the readout
+    face)."""
     nx, ny, nz = shape
     L = [float(box.L[i]) for i in range(3)]
     ax = [(np.arange(n, dtype=np.float64) + 0.5) * (L[i] / n) for i, n in enumerate((nx, ny, nz))]
+    if z_warp:
+        ax[2] = depth_unwarp((np.arange(nz, dtype=np.float64) + 0.5) / nz, z_warp) * L[2]
     z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
     return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1).astype(np.float32)
 
@@ -261,14 +286,22 @@ class LightSurrogate:
     members: list               # K parameter vectors (float32)
     cells: int = N_CELLS
     meta: dict = field(default_factory=dict)
+    z_warp: float = 0.0         # network input depth: 2 depth_warp(z / Lz) - 1
 
     def normalise(self, xyz: np.ndarray) -> np.ndarray:
-        return (2.0 * np.asarray(xyz, np.float32) / self.box_mm.astype(np.float32) - 1.0).astype(np.float32)
+        """Network inputs: x and y scaled to [-1, 1], z through the depth warp."""
+        q = np.asarray(xyz, np.float64).reshape(-1, 3)
+        L = self.box_mm.astype(np.float64)
+        out = 2.0 * q / L - 1.0
+        if self.z_warp:
+            out[:, 2] = 2.0 * depth_warp(q[:, 2] / L[2], self.z_warp) - 1.0
+        return out.astype(np.float32)
 
     @classmethod
     def train(cls, box: Box, xyz: np.ndarray, targets: np.ndarray, *, members: int = 5, steps: int = 20000,
               batch: int = 65536, lr: float = 1e-3, lr_final: Optional[float] = None,
-              time_weight: float = 1.0, seed: int = 0, device: int = 0, chunk: int = 250, log=None):
+              time_weight: float = 1.0, z_warp: float = 0.0, seed: int = 0, device: int = 0,
+              chunk: int = 250, log=None):
         """Train ``members`` networks on standardised targets.
 
         ``lr_final``: cosine decay of the Adam step size from ``lr`` to
@@ -283,7 +316,7 @@ class LightSurrogate:
         y_mean = targets.mean(0).astype(np.float64)
         y_std = np.maximum(targets.std(0), 1e-6).astype(np.float64)
         y_std[N_CELLS:] /= math.sqrt(time_weight)
-        obj = cls(L, y_mean.astype(np.float32), y_std.astype(np.float32), [])
+        obj = cls(L, y_mean.astype(np.float32), y_std.astype(np.float32), [], z_warp=float(z_warp))
         x = torch.from_numpy(obj.normalise(xyz)).to(f"cuda:{device}")
         y = torch.from_numpy(((targets - y_mean) / y_std).astype(np.float32)).to(f"cuda:{device}")
         history = []
@@ -306,7 +339,7 @@ class LightSurrogate:
             history.append(hist)
             net.close()
         obj.meta = {"steps": steps, "batch": batch, "lr": lr, "lr_final": lr_final,
-                    "time_weight": time_weight, "seed": seed,
+                    "time_weight": time_weight, "z_warp": z_warp, "seed": seed,
                     "train_seconds": time.perf_counter() - t0, "loss_history": history}
         return obj
 
@@ -338,11 +371,11 @@ class LightSurrogate:
 
     def save(self, path: str):
         np.savez_compressed(path, box_mm=self.box_mm, y_mean=self.y_mean, y_std=self.y_std,
-                            members=np.stack(self.members), cells=self.cells,
+                            members=np.stack(self.members), cells=self.cells, z_warp=np.float64(self.z_warp),
                             meta=np.array(repr({k: v for k, v in self.meta.items() if k != "loss_history"})))
 
     @classmethod
     def load(cls, path: str):
         z = np.load(path, allow_pickle=False)
         return cls(z["box_mm"], z["y_mean"], z["y_std"], list(z["members"]), int(z["cells"]),
-                   {"saved": str(z["meta"])})
+                   {"saved": str(z["meta"])}, float(z["z_warp"]) if "z_warp" in z.files else 0.0)

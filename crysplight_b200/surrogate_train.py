@@ -100,6 +100,8 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--lr-final", type=float, default=1e-5,
                     help="cosine decay of the step size to this value (negative: constant lr)")
+    ap.add_argument("--z-warp", type=float, default=0.0,
+                    help="depth warp of the grid and of the network input (0 = uniform in z)")
     ap.add_argument("--time-weight", type=float, default=0.1,
                     help="loss weight of the arrival-time outputs relative to the probabilities")
     ap.add_argument("--seed", type=int, default=4242)
@@ -119,8 +121,8 @@ def main(argv=None):
     eng = Engine(args.device)
     rep = {"setup": args.setup, "grid": list(args.grid), "photons_per_point": args.photons,
            "members": args.members, "steps": args.steps, "batch": args.batch, "lr": args.lr,
-           "lr_final": args.lr_final, "time_weight": args.time_weight}
-    pts = grid_points(box, tuple(args.grid))
+           "lr_final": args.lr_final, "time_weight": args.time_weight, "z_warp": args.z_warp}
+    pts = grid_points(box, tuple(args.grid), z_warp=args.z_warp)
     scan = scan_light(eng, box, op, ro, points=pts, photons_per_point=args.photons, seed=args.seed)
     n_ph = pts.shape[0] * args.photons
     rep["scan"] = {"points": int(pts.shape[0]), "photons": n_ph, "seconds": scan.seconds,
@@ -135,7 +137,8 @@ def main(argv=None):
         sur = LightSurrogate.train(box, pts[tr], y[tr], members=args.members, steps=args.steps,
                                    batch=args.batch, lr=args.lr,
                                    lr_final=args.lr_final if args.lr_final >= 0 else None,
-                                   time_weight=args.time_weight, seed=args.seed, device=args.device,
+                                   time_weight=args.time_weight, z_warp=args.z_warp, seed=args.seed,
+                                   device=args.device,
                                    log=lambda s: print(s, flush=True))
         rep["train_seconds"] = sur.meta["train_seconds"]
         rep["final_loss"] = [h[-1] for h in sur.meta["loss_history"]]

@@ -314,6 +314,17 @@ int cl_surrogate_combine(const float* d_raw, int32_t members, int64_t n_sites,
                          uint8_t* d_flag, void* stream);
 
 /*
+ * Network inputs of the surrogate for n_sites emission points (no counterpart
+ * in the reference): d_out[i] = (2x/Lx - 1, 2y/Ly - 1, 2w - 1) for
+ * d_xyz[i] = (x, y, z) in mm, with the depth warp
+ * w = (1 - z_warp) t + z_warp (1 - sqrt(1 - t)), t = z/Lz clamped to [0, 1]
+ * (z_warp in [0, 1]; the readout face is z = Lz).  Device arrays [n][3],
+ * asynchronous on `stream`; allocates nothing.
+ */
+int cl_surrogate_inputs(const float* d_xyz, int64_t n_sites, const cl_box* box, float z_warp,
+                        float* d_out, void* stream);
+
+/*
  * Diagnostics for tests: n draws (stream i = draw i, key = seed) of the
  * surrogate sampler's variates into device memory: fn 0 = binomial
  * (n = par[0], p = par[1]) -> int64; fn 1 = minimum of k = par[0] arrival
