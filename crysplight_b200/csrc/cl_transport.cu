@@ -1420,11 +1420,19 @@ int cl_debug_eval(cl_handle* h, int fn, const void* in, void* out, int64_t n, ui
 {
     if (!h) return CL_ERR_STATE;
     h->err[0] = 0;
-    if (n < 0 || !out || (fn != 4 && !in)) return set_err(h, CL_ERR_ARG, "bad debug arguments");
-    if (fn < 0 || fn > 5) return set_err(h, CL_ERR_ARG, "unknown debug function");
+    if (n < 0 || !out || (fn != 4 && fn != 6 && !in)) return set_err(h, CL_ERR_ARG, "bad debug arguments");
+    if (fn < 0 || fn > 6) return set_err(h, CL_ERR_ARG, "unknown debug function");
     if (fn == 4 && n_per < 1) return set_err(h, CL_ERR_ARG, "n_per must be >= 1");
     CK(h, cudaSetDevice(h->device), "cudaSetDevice");
     cudaStream_t st = h->stream;
+    if (fn == 6) {
+        // the handle's table of the logs of the uniforms (2^24 floats)
+        if (!h->logtab.p) return set_err(h, CL_ERR_STATE, "this handle has no log table");
+        if (n > (1 << 24)) return set_err(h, CL_ERR_ARG, "the log table has 2^24 entries");
+        CK(h, cudaMemcpyAsync(out, h->logtab.p, 4 * (size_t)n, cudaMemcpyDeviceToHost, st), "copy table");
+        CK(h, cudaStreamSynchronize(st), "stream synchronize");
+        return CL_OK;
+    }
     size_t in_b = 0, out_b = 0;
     if (fn <= 2) { in_b = 4 * (size_t)n; out_b = 4 * (size_t)n; }
     else if (fn == 3 || fn == 5) { in_b = 16 * (size_t)n; out_b = 16 * (size_t)n; }

@@ -226,6 +226,12 @@ class Engine:
         self._check(self.lib.cl_debug_eval(self.handle, code, _ptr(x), _ptr(out), x.size, 0, 0))
         return out
 
+    def log_table(self, n: int = 1 << 24) -> np.ndarray:
+        """The transport's table of log((k+1) 2^-24), k < n (float32)."""
+        out = np.empty(int(n), np.float32)
+        self._check(self.lib.cl_debug_eval(self.handle, 6, None, _ptr(out), int(n), 0, 0))
+        return out
+
     def philox(self, ctr: np.ndarray, seed: int, use_curand: bool = False) -> np.ndarray:
         ctr = np.ascontiguousarray(ctr, dtype=np.uint32).reshape(-1, 4)
         out = np.empty_like(ctr)

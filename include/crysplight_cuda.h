@@ -358,7 +358,9 @@ int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta,
  * on n inputs.  fn: 0 = log, 1 = sin, 2 = cos, 3 = Philox4x32-10 on
  * (in_u32[4k..4k+3] counter, key = (seed lo, hi)) -> out_u32[4k..4k+3],
  * 4 = randu stream: out[k*m + i] = i-th uniform of pid = k + 1 (m = n_per),
- * 5 = cuRAND's Philox4x32-10 on the same inputs as 3 (cross-check).
+ * 5 = cuRAND's Philox4x32-10 on the same inputs as 3 (cross-check),
+ * 6 = the first n entries of the handle's table of logs of the uniforms,
+ * out_f32[k] = log((k+1) * 2^-24) as the transport uses it (in unused).
  * Host buffers, synchronous.
  */
 int cl_debug_eval(cl_handle* h, int fn, const void* in, void* out, int64_t n,

@@ -72,6 +72,16 @@ def test_log_exhaustive_over_uniforms(engine, oracle):
     assert bad.size == 0
 
 
+def test_log_table_exhaustive(engine, oracle):
+    """The table the transport reads its logs from holds the oracle's bits
+    for all 2^24 uniforms."""
+    tab = engine.log_table()
+    ref = oracle.eval_math("log", ALL_RANDU)
+    bad = np.flatnonzero(tab.view(np.uint32) != ref.view(np.uint32))
+    print("log table mismatches:", bad.size)
+    assert bad.size == 0
+
+
 def test_sincos_exhaustive_over_azimuths(engine, oracle):
     """All 2^24 azimuths (2f0*Float32(pi))*u."""
     phi = (np.float32(2.0) * np.float32(math.pi)) * ALL_RANDU
