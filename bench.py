@@ -51,10 +51,14 @@ import numpy as np
 # instrumented oracle (python -m oracle.opcount).
 OPS_PER_STEP = {"scan256": 165.6, "point1m": 186.7}
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (read + write) per launch of the transport kernel from ncu
-# (profiles/transport_kernel_*.md); independent of the photon count: the only
-# DRAM traffic is the sources, offsets and output maps.
-TRAFFIC_BYTES = {"scan256": 244_224, "point1m": 82_944}
+# DRAM bytes (read + write) per launch of the transport kernel: one ncu capture
+# of the scan at 20,000 photons per point (profiles/transport_kernel_scan256x20k.md,
+# 2.99 GB for 494.8M photon-steps) scaled to the full launch by photon-steps.
+# Almost all of it is L2 misses of the 64 MB log table (about 2 bytes per
+# photon-step x log lookup), which grow in proportion to the steps; the
+# sources, offsets and maps are 0.24 MB.  point1m: not captured.
+TRAFFIC_PER_STEP = 2.991583e9 / 494_804_727
+TRAFFIC_BYTES = {"point1m": None}
 
 
 def events_workload(n_events: int = 50_000):
@@ -572,7 +576,9 @@ def run_cuda_arm(args, W, rank, world, local_rank):
         "photon_steps_per_s": steps_per_launch / launch_s,
         "roofline": {
             "bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gop/s",
-            "frac": achieved / peak, "traffic": TRAFFIC_BYTES.get(W["name"]),
+            "frac": achieved / peak,
+            "traffic": (TRAFFIC_PER_STEP * steps_per_launch if W["name"] == "scan256"
+                        else TRAFFIC_BYTES.get(W["name"])),
             "ops_per_step": ops_step,
             "note": ("reference Float32/int ops per photon-step x steps / launch time, against "
                      "one op per lane per clock (SMs x 128 lanes x max SM clock of measured)"),
