@@ -33,8 +33,9 @@ import numpy as np
 
 from . import _lib
 from .events import EventsResult, GammaMaterial, gamma_stage
-from .params import COUNTER_NAMES, Box, Counters, OpticalParams, Readout, TimeBinning
+from .params import COUNTER_NAMES, Box, OpticalParams, Readout, TimeBinning
 from .surrogate import D_OUT, MLP, N_CELLS, LightSurrogate
+from .transport import stream_arg
 
 SPREAD_MAX = 0.02
 WALL_MIN_MM = 1.0
@@ -87,7 +88,7 @@ class SurrogateEvents:
         xin = torch.empty((n, 3), dtype=torch.float32, device=self.dev)
         rc = self.lib.cl_surrogate_inputs(C.c_void_p(xyz.data_ptr()), n, C.byref(self.box),
                                           float(self.sur.z_warp), C.c_void_p(xin.data_ptr()),
-                                          C.c_void_p(stream) if stream else None)
+                                          stream_arg(stream))
         if rc != 0:
             raise _lib.CudaTransportError(rc, "cl_surrogate_inputs failed")
         torch.cuda.synchronize(self.dev)         # the networks run on their own streams
@@ -105,7 +106,7 @@ class SurrogateEvents:
             P(raw.data_ptr()), K, n, P(self.y_mean.data_ptr()), P(self.y_std.data_ptr()),
             P(xyz.data_ptr()), C.byref(self.box), C.byref(ro), float(pde), float(spread_max),
             float(wall_min_mm), P(out.p.data_ptr()), P(out.tmean.data_ptr()), P(out.tsig.data_ptr()),
-            P(out.spread.data_ptr()), P(out.flag.data_ptr()), P(stream) if stream else None)
+            P(out.spread.data_ptr()), P(out.flag.data_ptr()), stream_arg(stream))
         if rc != 0:
             raise _lib.CudaTransportError(rc, "cl_surrogate_combine failed")
         return out
@@ -184,6 +185,8 @@ def sample_sites(engine, box: Box, op: OpticalParams, ro: Readout, tb: TimeBinni
     ro = ro if isinstance(ro, Readout) else Readout(ro)
     if stream:
         torch.cuda.ExternalStream(stream, device=dev).synchronize()
+    else:
+        torch.cuda.synchronize(dev)
     flag_h = light.flag.cpu().numpy()          # the host picks the fallback sites
     fb = np.nonzero(flag_h)[0]
     n_sites = int(xyz.shape[0])
@@ -216,7 +219,7 @@ def sample_sites(engine, box: Box, op: OpticalParams, ro: Readout, tb: TimeBinni
         ptr(light.p), ptr(light.tmean), ptr(light.tsig), ptr(light.flag), ptr(t0.contiguous()),
         ptr(photons.contiguous()), ptr(segment.contiguous()), n_sites, int(seed) & 0xFFFFFFFFFFFFFFFF,
         int(n_segments), ptr(maps), ptr(tmin), ptr(npe), ptr(ctr), ptr(sampled),
-        P(stream) if stream else None)
+        stream_arg(stream))
     eng._check(rc)
     eng.sync(stream)
     stats = {"sites": n_sites, "fallback_sites": int(fb.size), "photons_mc": n_mc,

@@ -20,7 +20,7 @@ runs with the CUDA engine or, in tests, on the CPU.
 """
 from __future__ import annotations
 
-from typing import Callable, Optional, Sequence
+from typing import Callable, Sequence
 
 import numpy as np
 

@@ -16,7 +16,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from .params import Box, Counters, Readout, TimeBinning
+from .params import Box, Readout, TimeBinning
 
 D_IN, D_H, D_OUT = 3, 256, 192
 N_CELLS = 64

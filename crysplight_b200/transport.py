@@ -26,6 +26,20 @@ def _ptr(a: Optional[np.ndarray]):
     return None if a is None else C.c_void_p(a.ctypes.data)
 
 
+# cudaStreamLegacy: the legacy default stream, named explicitly because the
+# C-ABI reads a NULL stream as the handle's own stream.
+CUDA_STREAM_LEGACY = 1
+
+
+def stream_arg(stream):
+    """The C-ABI stream argument for a CUDA stream handle: None -> NULL (the
+    library handle's stream); 0, torch's default stream -> cudaStreamLegacy,
+    so that the call is ordered with the default stream's work."""
+    if stream is None:
+        return None
+    return C.c_void_p(int(stream) or CUDA_STREAM_LEGACY)
+
+
 def _as_readout(ro) -> Readout:
     return ro if isinstance(ro, Readout) else Readout(ro)
 
@@ -184,7 +198,7 @@ class Engine:
             C.c_void_p(px), C.c_void_p(py), C.c_void_p(pz), C.c_void_p(pt) if pt else None,
             int(npos), int(n_photons), int(seed), int(pid_offset), float(np.float32(tau_ns)),
             int(max_bounces), C.c_void_p(counts), C.c_void_p(first_ns), C.c_void_p(counters),
-            None, C.c_void_p(stream) if stream else None)
+            None, stream_arg(stream))
         self._check(rc)
 
     def run_segments_device(self, box, op, ro, tb, *, sx, sy, sz, st, src_offsets, src_segment,
@@ -197,7 +211,7 @@ class Engine:
             C.c_void_p(src_offsets), C.c_void_p(src_segment), int(n_src), int(n_segments),
             int(n_photons), int(seed), int(pid_offset), float(np.float32(tau_ns)), int(max_bounces),
             C.c_void_p(maps), C.c_void_p(tmin), C.c_void_p(npe), C.c_void_p(counters), None,
-            C.c_void_p(stream) if stream else None)
+            stream_arg(stream))
         self._check(rc)
 
     def run_segments_moments_device(self, box, op, ro, tb, *, sx, sy, sz, st, src_offsets, src_segment,
@@ -212,11 +226,11 @@ class Engine:
             C.c_void_p(src_offsets), C.c_void_p(src_segment), int(n_src), int(n_segments),
             int(n_photons), int(seed), int(pid_offset), float(np.float32(tau_ns)), int(max_bounces),
             C.c_void_p(maps), C.c_void_p(tmin), C.c_void_p(npe), C.c_void_p(counters),
-            C.c_void_p(tsum), C.c_void_p(tsum2), C.c_void_p(stream) if stream else None)
+            C.c_void_p(tsum), C.c_void_p(tsum2), stream_arg(stream))
         self._check(rc)
 
     def sync(self, stream=None) -> None:
-        self._check(self.lib.cl_sync(self.handle, C.c_void_p(stream) if stream else None))
+        self._check(self.lib.cl_sync(self.handle, stream_arg(stream)))
 
     # -- diagnostics -----------------------------------------------------------
     def eval_math(self, fn: str, x: np.ndarray) -> np.ndarray:
