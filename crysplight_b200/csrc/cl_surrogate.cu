@@ -27,7 +27,8 @@
 // (whose fourth counter word is 0).
 //
 // Every loop is bounded; a budget that runs out sets bit 2 of the error word
-// and the site's remaining draws fall back to the mean.
+// and the site's remaining draws fall back to the mean.  A site whose segment
+// id lies outside the maps is skipped and sets bit 3.
 #include <cmath>
 #include <cstdint>
 
@@ -224,14 +225,16 @@ __global__ void __launch_bounds__(128) surrogate_sample(const SurSampleArgs A)
         if (A.flag && A.flag[i]) continue;
         int64_t left = A.photons[i];
         if (left <= 0) continue;
-        ph += (unsigned long long)left;
         Uni U;
         U.init((uint64_t)i, A.k0, A.k1);
         const float* p = A.p + i * A.cells;
         const float* tm = A.tmean + i * A.cells;
         const float* ts = A.tsig + i * A.cells;
         const double t0 = (double)A.t0[i];
-        const int64_t base = (int64_t)A.seg[i] * A.cells;
+        const int32_t sg = A.seg[i];
+        if (sg < 0 || (int64_t)sg >= A.n_seg) { bad |= 8u; continue; }
+        ph += (unsigned long long)left;
+        const int64_t base = (int64_t)sg * A.cells;
         double mass = 1.0;                          // probability not yet assigned
         for (int c = 0; c < A.cells && left > 0; ++c) {
             const double pc = (double)p[c];

@@ -20,13 +20,14 @@ struct SurSampleArgs {
     const int64_t* photons;  // [n] photons emitted by the site
     const int32_t* seg;      // [n] segment (event) index
     int64_t n;
+    int64_t n_seg;           // segments in maps / keys (sites outside are skipped, bit 3 of err)
     int32_t cells;
     uint32_t k0, k1;         // Philox key (seed)
     float tau;               // scintillation decay time (ns), 0 = prompt
     uint32_t* maps;          // [n_seg][cells] counts
     uint32_t* keys;          // [n_seg][cells] order-preserving time keys
     unsigned long long* stats;  // [2] += photons of sampled sites, sampled detections (may be NULL)
-    unsigned int* err;       // bit 2 set if a sampler loop budget ran out
+    unsigned int* err;       // bit 2: a sampler loop budget ran out; bit 3: a segment id out of range
 };
 
 // Enqueue the sampler on `st`; returns a cudaError_t of the launch.

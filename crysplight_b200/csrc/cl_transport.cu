@@ -1108,6 +1108,7 @@ static int collect(cl_handle* h, cudaStream_t st)
     CK(h, cudaStreamSynchronize(st), "stream synchronize");
     h->last_steps = (int64_t)steps;
     if (err & 2u) return set_err(h, CL_ERR_CUDA, "internal error: uniform ring underflow in the transport kernel");
+    if (err & 8u) return set_err(h, CL_ERR_ARG, "a surrogate site's segment id is out of range (site skipped)");
     if (err & 4u) return set_err(h, CL_ERR_TIMEOUT, "a loop budget of the surrogate sampler ran out");
     if (err) return set_err(h, CL_ERR_TIMEOUT, "a device-side loop budget ran out (Rayleigh rejection sampler)");
     return CL_OK;
@@ -1398,6 +1399,7 @@ int cl_run_events_surrogate_device(cl_handle* h, const cl_box* box, const cl_opt
     memset(&sa, 0, sizeof sa);
     sa.p = d_site_p; sa.tmean = d_site_tmean; sa.tsig = d_site_tsig; sa.flag = d_site_flag;
     sa.t0 = d_site_t0; sa.photons = d_site_photons; sa.seg = d_site_segment; sa.n = n_sites;
+    sa.n_seg = n_segments;
     sa.cells = ro->grid.nx * ro->grid.ny;
     sa.k0 = (uint32_t)sample_seed; sa.k1 = (uint32_t)(sample_seed >> 32);
     sa.tau = tau_ns;

@@ -277,7 +277,9 @@ int cl_run_segments_moments_device(cl_handle* h,
  * Sampler uniforms: Philox4x32-10 keyed by sample_seed, a stream per site.
  * d_counters count the Monte Carlo photons only; d_sampled (uint64[2], may be
  * NULL) gets the photons of sampled sites and their sampled detections.
- * Asynchronous; cl_sync reports CL_ERR_TIMEOUT if a sampler loop budget ran out.
+ * Asynchronous; cl_sync reports CL_ERR_TIMEOUT if a sampler loop budget ran
+ * out and CL_ERR_ARG if a sampled site's segment id lay outside
+ * [0, n_segments) (that site is skipped).
  */
 int cl_run_events_surrogate_device(cl_handle* h,
                                    const cl_box* box, const cl_optical_params* op,

@@ -68,3 +68,30 @@ def test_mlp_rejects_bad_batches():
         assert np.isfinite(m.train(2, batch=128))
     finally:
         m.close()
+
+
+def test_sampled_site_with_a_bad_segment_is_skipped_and_reported(engine):
+    """A device-side segment id outside the maps is caught in the sampler
+    kernel (no out-of-range write) and reported by the sync."""
+    import torch
+    from crysplight_b200 import _lib
+    from crysplight_b200.fast_events import SiteLight, sample_sites
+    from crysplight_b200._lib import CudaTransportError
+    n = 4
+    xyz = torch.full((n, 3), 10.0, device="cuda")
+    t0 = torch.zeros(n, device="cuda")
+    ph = torch.full((n,), 1000, dtype=torch.int64, device="cuda")
+    seg = torch.tensor([0, 1, 7, 1], dtype=torch.int32, device="cuda")      # 7 >= n_segments
+    p = torch.full((n, 64), 0.004, device="cuda")
+    light = SiteLight(p, torch.full((n, 64), 2.0, device="cuda"), torch.full((n, 64), 0.5, device="cuda"),
+                      torch.zeros(n, device="cuda"), torch.zeros(n, dtype=torch.uint8, device="cuda"))
+    with pytest.raises(CudaTransportError) as e:
+        sample_sites(engine, BOX_BGO, OP_C2, GRID, TB80, xyz=xyz, t0=t0, photons=ph, segment=seg,
+                     n_segments=2, seed=3, tau_ns=1768.0, light=light)
+    assert e.value.code == _lib.CL_ERR_ARG and b"segment" in engine.lib.cl_last_error(engine.handle)
+    # valid ids go through afterwards
+    seg[2] = 0
+    (maps, tmin, npe, ctr, sampled), st = sample_sites(
+        engine, BOX_BGO, OP_C2, GRID, TB80, xyz=xyz, t0=t0, photons=ph, segment=seg, n_segments=2, seed=3,
+        tau_ns=1768.0, light=light)
+    assert int(sampled[0]) == 4000 and int(npe.sum()) == int(sampled[1]) > 0
