@@ -78,7 +78,7 @@ struct KArgs {
     int32_t cells;        // nx*ny
     int32_t bins_total;   // nbins+1
     const float* px; const float* py; const float* pz; const float* pt;
-    const int64_t* src_off; const int32_t* src_seg; int64_t n_src;
+    const int64_t* src_off; const int32_t* src_seg; int64_t n_src; int64_t n_seg;
     uint32_t* counts;     // point: cells*bins_total
     uint32_t* keys;       // point: cells; segments: cells*n_seg
     uint32_t* maps;       // segments: cells*n_seg
@@ -548,16 +548,23 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
                 if (lane == __ffs(g) - 1) atomicAdd(tile_counts + slot, (uint32_t)__popc(g));
                 atomicMin(tile_keys + cell, key);
             } else {
-                const unsigned long long slot =
-                    (unsigned long long)seg * (unsigned long long)A.cells + (unsigned long long)cell;
-                const unsigned g = __match_any_sync(dmask, slot);
-                if (lane == __ffs(g) - 1) atomicAdd(A.maps + slot, (uint32_t)__popc(g));
-                atomicMin(A.keys + slot, key);
-                if (MODE == 2) {
-                    // fixed-point time moments (exact integer sums, order-independent)
-                    const float tc = fminf(fmaxf(t, 0.0f), CL_MOMENT_T_MAX_NS);
-                    atomicAdd(A.tsum + slot, __float2ull_rn(tc * CL_MOMENT_T_SCALE));
-                    atomicAdd(A.tsum2 + slot, __float2ull_rn((tc * tc) * CL_MOMENT_T2_SCALE));
+                // a segment id outside the maps (untrusted device input) drops the detection
+                const bool seg_ok = seg >= 0 && (int64_t)seg < A.n_seg;
+                const unsigned okmask = __ballot_sync(dmask, seg_ok);
+                if (seg_ok) {
+                    const unsigned long long slot =
+                        (unsigned long long)seg * (unsigned long long)A.cells + (unsigned long long)cell;
+                    const unsigned g = __match_any_sync(okmask, slot);
+                    if (lane == __ffs(g) - 1) atomicAdd(A.maps + slot, (uint32_t)__popc(g));
+                    atomicMin(A.keys + slot, key);
+                    if (MODE == 2) {
+                        // fixed-point time moments (exact integer sums, order-independent)
+                        const float tc = fminf(fmaxf(t, 0.0f), CL_MOMENT_T_MAX_NS);
+                        atomicAdd(A.tsum + slot, __float2ull_rn(tc * CL_MOMENT_T_SCALE));
+                        atomicAdd(A.tsum2 + slot, __float2ull_rn((tc * tc) * CL_MOMENT_T2_SCALE));
+                    }
+                } else {
+                    atomicOr(A.err, 16u);
                 }
             }
         }
@@ -1074,7 +1081,7 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
         a.P = P; a.pid0 = pid0; a.n = n; a.npos = 1; a.warp_chunk = h->warp_chunk;
         a.cells = cells; a.bins_total = P.nbins + 1;
         a.px = sx; a.py = sy; a.pz = sz; a.pt = sT;
-        a.src_off = off; a.src_seg = segid; a.n_src = n_src;
+        a.src_off = off; a.src_seg = segid; a.n_src = n_src; a.n_seg = n_seg;
         a.keys = keys; a.maps = maps; a.counters = counters;
         const bool want_rec = rec && (rec->status || rec->idx || rec->t || rec->bounces);
         if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
@@ -1108,6 +1115,7 @@ static int collect(cl_handle* h, cudaStream_t st)
     CK(h, cudaStreamSynchronize(st), "stream synchronize");
     h->last_steps = (int64_t)steps;
     if (err & 2u) return set_err(h, CL_ERR_CUDA, "internal error: uniform ring underflow in the transport kernel");
+    if (err & 16u) return set_err(h, CL_ERR_ARG, "a source's segment id is out of range (its detections were dropped)");
     if (err & 8u) return set_err(h, CL_ERR_ARG, "a surrogate site's segment id is out of range (site skipped)");
     if (err & 4u) return set_err(h, CL_ERR_TIMEOUT, "a loop budget of the surrogate sampler ran out");
     if (err) return set_err(h, CL_ERR_TIMEOUT, "a device-side loop budget ran out (Rayleigh rejection sampler)");

@@ -95,3 +95,32 @@ def test_sampled_site_with_a_bad_segment_is_skipped_and_reported(engine):
         engine, BOX_BGO, OP_C2, GRID, TB80, xyz=xyz, t0=t0, photons=ph, segment=seg, n_segments=2, seed=3,
         tau_ns=1768.0, light=light)
     assert int(sampled[0]) == 4000 and int(npe.sum()) == int(sampled[1]) > 0
+
+
+def test_transport_source_with_a_bad_segment_is_reported(engine):
+    """cl_run_segments_device trusts its device arrays; a segment id outside
+    the maps still cannot write out of range: its detections are dropped and
+    the sync reports CL_ERR_ARG."""
+    import torch
+    from crysplight_b200 import _lib
+    from crysplight_b200._lib import CudaTransportError
+    dev = "cuda"
+    sx = torch.tensor([24.0, 24.0], device=dev)
+    sy = torch.tensor([24.0, 24.0], device=dev)
+    sz = torch.tensor([20.0, 20.0], device=dev)
+    off = torch.tensor([0, 500, 1000], dtype=torch.int64, device=dev)
+    seg = torch.tensor([0, 5], dtype=torch.int32, device=dev)           # 5 >= n_segments
+    maps = torch.zeros(64 * 2, dtype=torch.int32, device=dev)
+    tmin = torch.zeros(64 * 2, dtype=torch.float32, device=dev)
+    npe = torch.zeros(2, dtype=torch.int32, device=dev)
+    ctr = torch.zeros(9, dtype=torch.int64, device=dev)
+    st = torch.cuda.Stream()
+    engine.run_segments_device(BOX_BGO, OP_C2, GRID, TB80, sx=sx.data_ptr(), sy=sy.data_ptr(), sz=sz.data_ptr(),
+                               st=None, src_offsets=off.data_ptr(), src_segment=seg.data_ptr(), n_src=2,
+                               n_segments=2, n_photons=1000, seed=4, tau_ns=0.0, maps=maps.data_ptr(),
+                               tmin=tmin.data_ptr(), npe=npe.data_ptr(), counters=ctr.data_ptr(),
+                               stream=st.cuda_stream)
+    with pytest.raises(CudaTransportError) as e:
+        engine.sync(st.cuda_stream)
+    assert e.value.code == _lib.CL_ERR_ARG
+    assert int(maps[64:].sum()) == 0 and int(npe[0]) == int(maps[:64].sum()) > 0
