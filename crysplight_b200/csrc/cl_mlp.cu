@@ -19,6 +19,7 @@
 #include <new>
 #include <vector>
 
+#include <atomic>
 #include <mutex>
 
 #include <cuda.h>
@@ -380,11 +381,17 @@ int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, in
         return CL_ERR_ARG;
     CUtensorMap ta, tb;
     if (!make_map(&ta, A, g.M, g.K, lda, TILE_M) || !make_map(&tb, B, g.N, g.K, ldb, g.N)) return CL_ERR_ARG;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(gemm_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)gemm_smem_bytes(256));
-        attr_set = true;
+    // the shared-memory opt-in is a per-device attribute of the kernel: set it
+    // once for every device this process launches on
+    static std::atomic<uint64_t> attr_devices{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = 1ull << (dev & 63);
+    if (!(attr_devices.load() & bit)) {
+        if (cudaFuncSetAttribute(gemm_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)gemm_smem_bytes(256)) != cudaSuccess)
+            return CL_ERR_CUDA;
+        attr_devices.fetch_or(bit);
     }
     const int tiles = g.M / TILE_M;
     dim3 grid((unsigned)(grid_x < tiles ? grid_x : tiles), (unsigned)splits);
