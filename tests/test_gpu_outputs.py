@@ -75,3 +75,11 @@ def test_shoot_gammas_with_the_surrogate(engine, tmp_path):
     assert abs(d["npe"][peak].mean() / 2004.0 - 1) < 0.02        # the plain Monte Carlo's photopeak
     st = s["result"].surrogate_stats
     assert 0 < st["fallback_sites"] < st["sites"]
+
+
+def test_run_point_source_cli(tmp_path, capsys):
+    from crysplight_b200.run_point_source import main
+    cfg = _copy_run(tmp_path, "point_bgo_esr.toml")
+    main([cfg])
+    out = capsys.readouterr().out
+    assert "detected" in out and os.path.exists(tmp_path / "output" / "point_bgo_esr" / "light.h5")
