@@ -10,7 +10,7 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built sm_100a library")
-    config.addinivalue_line("markers", "slow: long-running (full BASELINE-size workloads)")
+    config.addinivalue_line("markers", "slow: long-running (full-size workloads)")
 
 
 def _have_gpu() -> bool:

@@ -281,7 +281,7 @@ def test_segments_equal_point_runs(engine):
         assert acc.ndet == res.npe[p]
 
 
-# ---- full BASELINE sizes: exact where the oracle is fast, properties otherwise -----------
+# ---- full workload sizes (10^6 photons; 51.2M photons): exact where the oracle is fast, properties otherwise
 def test_config1_full_size_exact(engine, oracle):
     """Config 1 at its full 1,000,000 photons: identical to the oracle."""
     kw = dict(n_photons=1_000_000, seed=1234, pos=CENTRE_CSI, tau_ns=TAU_C1)
