@@ -424,14 +424,18 @@ __device__ __forceinline__ uint32_t hash32(uint32_t a, uint32_t b, uint32_t c)
 }
 
 // Random minibatch (with replacement) from the training set.
-__global__ void gather_batch(const float* __restrict__ X, const float* __restrict__ T, int64_t n_all,
-                             int B, uint32_t seed, uint32_t step, float* Xb, float* Tb)
+__global__ void __launch_bounds__(256) gather_batch(const float* __restrict__ X, const float* __restrict__ T,
+                                                    int64_t n_all, int B, uint32_t seed, uint32_t step,
+                                                    float* Xb, float* Tb)
 {
-    const int b = blockIdx.x;
+    // one warp per row: the target row (192 floats) as 48 float4
+    const int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (b >= B) return;
     const int64_t i = (int64_t)(hash32((uint32_t)b, step, seed) % (uint32_t)n_all);
-    if (threadIdx.x < D_IN) Xb[(int64_t)b * D_IN + threadIdx.x] = X[i * D_IN + threadIdx.x];
-    for (int j = threadIdx.x; j < D_OUT; j += blockDim.x) Tb[(int64_t)b * D_OUT + j] = T[i * D_OUT + j];
+    if (lane < D_IN) Xb[(int64_t)b * D_IN + lane] = X[i * D_IN + lane];
+    const float4* src = reinterpret_cast<const float4*>(T + i * D_OUT);
+    float4* dst = reinterpret_cast<float4*>(Tb + (int64_t)b * D_OUT);
+    for (int j = lane; j < D_OUT / 4; j += 32) dst[j] = src[j];
 }
 
 // Layer 1 (K = 3) on the CUDA cores: h = silu(x W1^T + b1) for 64 rows per
@@ -478,25 +482,37 @@ __global__ void reduce_wgrad(const float* __restrict__ P, int S, int IN, int OUT
 // Adam on an FP32 master tensor; optional BF16 copies of a [OUT][IN] matrix
 // in both layouts ([OUT][IN] for the forward B operand, [IN][OUT] for the
 // backward-data B operand).
-__global__ void adam_step(float* w, const float* g, float* m, float* v, int n, float lr, float b1,
-                          float b2, float eps, float bc1, float bc2, int OUT, int IN, bf16* wt_bf,
-                          bf16* w_bf)
+// Adam over the whole parameter block in one launch; the three weight
+// matrices of the tensor-core layers also get their BF16 copies (W^T as
+// stored and W), described by AdamCopies.
+struct AdamCopies {
+    int64_t off[3]; int n[3]; int OUT[3]; int IN[3];
+    bf16* wt[3]; bf16* w[3];
+};
+__global__ void adam_all(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                         float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps, float bc1,
+                         float bc2, const AdamCopies C)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float gi = g[i];
-    const float mi = b1 * m[i] + (1.0f - b1) * gi;
-    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-    m[i] = mi; v[i] = vi;
-    const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
-    w[i] = wi;
-    if (wt_bf) {
-        const int o = i / IN, k = i % IN;
-        const bf16 q = __float2bfloat16_rn(wi);
-        wt_bf[i] = q;
-        w_bf[(int64_t)k * OUT + o] = q;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi; v[i] = vi;
+        const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+        w[i] = wi;
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const int64_t r = i - C.off[t];
+            if (r >= 0 && r < C.n[t]) {
+                const int o = (int)(r / C.IN[t]), k = (int)(r % C.IN[t]);
+                const bf16 q = __float2bfloat16_rn(wi);
+                C.wt[t][r] = q;
+                C.w[t][(int64_t)k * C.OUT[t] + o] = q;
+            }
+        }
     }
 }
+
 
 __global__ void to_bf16_pair(const float* w, int OUT, int IN, bf16* wt_bf, bf16* w_bf)
 {
@@ -660,18 +676,17 @@ void adam(cl_mlp* m, float lr, cudaStream_t st)
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     m->adam_t += 1;
     const float bc1 = 1.0f - powf(b1, (float)m->adam_t), bc2 = 1.0f - powf(b2, (float)m->adam_t);
-    struct T { int64_t off; int n; int OUT; int IN; bf16* wt; bf16* w; };
-    const T ts[8] = {{OFF_W1, D_H * D_IN, 0, 0, nullptr, nullptr},
-                     {OFF_B1, D_H, 0, 0, nullptr, nullptr},
-                     {OFF_W2, D_H * D_H, D_H, D_H, m->w2t, m->w2},
-                     {OFF_B2, D_H, 0, 0, nullptr, nullptr},
-                     {OFF_W3, D_H * D_H, D_H, D_H, m->w3t, m->w3},
-                     {OFF_B3, D_H, 0, 0, nullptr, nullptr},
-                     {OFF_W4, D_OUT * D_H, D_OUT, D_H, m->w4t, m->w4},
-                     {OFF_B4, D_OUT, 0, 0, nullptr, nullptr}};
-    for (const T& t : ts)
-        adam_step<<<(t.n + 255) / 256, 256, 0, st>>>(m->p + t.off, m->g + t.off, m->m + t.off, m->v + t.off,
-                                                     t.n, lr, b1, b2, eps, bc1, bc2, t.OUT, t.IN, t.wt, t.w);
+    AdamCopies c;
+    const int64_t offs[3] = {OFF_W2, OFF_W3, OFF_W4};
+    const int outs[3] = {D_H, D_H, D_OUT};
+    bf16* wts[3] = {m->w2t, m->w3t, m->w4t};
+    bf16* ws[3] = {m->w2, m->w3, m->w4};
+    for (int t = 0; t < 3; ++t) {
+        c.off[t] = offs[t]; c.OUT[t] = outs[t]; c.IN[t] = D_H; c.n[t] = outs[t] * D_H;
+        c.wt[t] = wts[t]; c.w[t] = ws[t];
+    }
+    const unsigned grid = (unsigned)((N_PARAMS + 255) / 256);
+    adam_all<<<grid, 256, 0, st>>>(m->p, m->g, m->m, m->v, N_PARAMS, lr, b1, b2, eps, bc1, bc2, c);
 }
 
 }  // namespace
@@ -789,7 +804,7 @@ int cl_mlp_train(cl_mlp* m, int steps, int batch, float lr, uint32_t seed, uint3
     cudaStream_t st = m->stream;
     cudaMemsetAsync(m->loss, 0, sizeof(float), st);
     for (int s = 0; s < steps; ++s) {
-        gather_batch<<<batch, 64, 0, st>>>(m->data_x, m->data_t, m->n_data, batch, seed, step0 + (uint32_t)s,
+        gather_batch<<<(batch + 7) / 8, 256, 0, st>>>(m->data_x, m->data_t, m->n_data, batch, seed, step0 + (uint32_t)s,
                                           m->xb, m->tb);
         int rc = forward(m, batch, true, st);
         if (!rc) rc = backward(m, batch, st);
