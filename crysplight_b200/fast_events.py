@@ -162,10 +162,12 @@ class SurrogateEvents:
         (maps, tmin, npe, ctr, sampled), stats = self.transport_sites(
             box, op, ro, tb, xyz=xyz, t0=t0, photons=ph, segment=seg, n_segments=n, seed=seed,
             tau_ns=tau_ns, max_bounces=max_bounces, spread_max=spread_max, wall_min_mm=wall_min_mm)
-        m = maps.cpu().numpy().view(np.uint32)
-        out.maps[...] = (m & 0xFFFF).astype(np.uint16).reshape((nx, ny, n), order="F")
-        out.tmin[...] = tmin.cpu().numpy().reshape((nx, ny, n), order="F")
-        out.npe[...] = npe.cpu().numpy()
+        # the device maps are [event][cell], the memory order of the Fortran
+        # (nx, ny, n) arrays: copy straight into them (UInt16 maps wrap as in Julia)
+        torch.from_numpy(out.maps.reshape(-1, order="F").view(np.int16)).copy_(
+            (maps & 0xFFFF).to(torch.int16))
+        torch.from_numpy(out.tmin.reshape(-1, order="F")).copy_(tmin)
+        torch.from_numpy(out.npe).copy_(npe)
         out.n_photons = g.n_photons
         out.counters = dict(zip(COUNTER_NAMES, (int(v) for v in ctr.cpu().numpy())))
         s = sampled.cpu().numpy()
