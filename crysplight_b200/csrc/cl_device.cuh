@@ -395,14 +395,22 @@ __device__ __forceinline__ void specular(float& ux, float& uy, float& uz, int32_
     if (a == 1) ux = -ux; else if (a == 2) uy = -uy; else uz = -uz;
 }
 
+// Distance along one axis to the face the direction points at:
+// u > 0 ? (L - p) / u : (u < 0 ? -p / u : Inf).  The numerator is selected
+// first, so a warp whose lanes point both ways runs one division, not two.
+__device__ __forceinline__ float axis_distance(float L, float p, float u)
+{
+    const float q = (u > 0.0f ? L - p : -p) / u;
+    return (u > 0.0f || u < 0.0f) ? q : __int_as_float(0x7f800000);
+}
+
 // wall_hit, src/geometry.jl:19-32.
 __device__ __forceinline__ int32_t wall_hit(const Physics& P, float x, float y, float z,
                                             float ux, float uy, float uz, float& d)
 {
-    const float inf = __int_as_float(0x7f800000);
-    const float dx = ux > 0.0f ? (P.L0 - x) / ux : (ux < 0.0f ? (-x) / ux : inf);
-    const float dy = uy > 0.0f ? (P.L1 - y) / uy : (uy < 0.0f ? (-y) / uy : inf);
-    const float dz = uz > 0.0f ? (P.L2 - z) / uz : (uz < 0.0f ? (-z) / uz : inf);
+    const float dx = axis_distance(P.L0, x, ux);
+    const float dy = axis_distance(P.L1, y, uy);
+    const float dz = axis_distance(P.L2, z, uz);
     if (dx <= dy && dx <= dz) { d = dx; return ux > 0.0f ? FACE_XP : FACE_XM; }
     if (dy <= dz)             { d = dy; return uy > 0.0f ? FACE_YP : FACE_YM; }
     d = dz;
@@ -433,14 +441,15 @@ __device__ __forceinline__ void rayleigh_rotate(float mu, float sphi, float cphi
 {
     const float st = sqrtf(fmaxf(0.0f, 1.0f - mu * mu));
     const float cb = st * cphi, sb = st * sphi;
-    float t1x, t1y, t1z, inv;
-    if (fabsf(uz) < 0.9f) {
-        inv = 1.0f / sqrtf(ux * ux + uy * uy);
-        t1x = -uy * inv; t1y = ux * inv; t1z = 0.0f;
-    } else {
-        inv = 1.0f / sqrtf(uy * uy + uz * uz);
-        t1x = 0.0f; t1y = -uz * inv; t1z = uy * inv;
-    }
+    // t1 = (-uy, ux, 0)/|(ux, uy)| if |uz| < 0.9, else (0, -uz, uy)/|(uy, uz)|:
+    // the same operations on selected operands (one square root and division
+    // for a warp whose lanes take both cases)
+    const bool zlow = fabsf(uz) < 0.9f;
+    const float pa = zlow ? ux : uy, pb = zlow ? uy : uz;
+    float inv = 1.0f / sqrtf(pa * pa + pb * pb);
+    const float t1x = zlow ? -pb * inv : 0.0f;
+    const float t1y = zlow ? pa * inv : -pb * inv;
+    const float t1z = zlow ? 0.0f : pa * inv;
     const float t2x = uy * t1z - uz * t1y;
     const float t2y = uz * t1x - ux * t1z;
     const float t2z = ux * t1y - uy * t1x;
