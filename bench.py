@@ -152,6 +152,8 @@ def surrogate_training_bench(dev, steps: int = 200, warmup: int = 20) -> dict:
 
 
 SURROGATE_BGO = os.path.join(ROOT, "crysplight_b200", "surrogates", "bgo_esr.npz")
+# the expert ensemble of the last millimetres before the readout face (used when present)
+SURROGATE_BGO_FACE = os.path.join(ROOT, "crysplight_b200", "surrogates", "bgo_esr_face.npz")
 
 
 def surrogate_events_workload(n_events: int = 500_000):
@@ -171,7 +173,8 @@ def surrogate_events_workload(n_events: int = 500_000):
                      "from a wrapped face)")
 
 
-def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wall_min_mm=1.0):
+def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wall_min_mm=1.0,
+                               expert: bool = True):
     """events/s of the surrogate + fallback pipeline with the deposits in HBM
     (value), the plain Monte Carlo on the same deposits, their agreement, and
     the whole public call SurrogateEvents.run_events (e2e)."""
@@ -180,7 +183,8 @@ def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wal
     from crysplight_b200.fast_events import SurrogateEvents, compare_maps, photopeak
     from crysplight_b200.surrogate import LightSurrogate
     sur = LightSurrogate.load(SURROGATE_BGO)
-    se = SurrogateEvents(sur, eng, device=dev.index or 0)
+    experts = [LightSurrogate.load(SURROGATE_BGO_FACE)] if expert and os.path.exists(SURROGATE_BGO_FACE) else []
+    se = SurrogateEvents(sur, eng, device=dev.index or 0, experts=experts)
     g = gamma_stage(E["mat"], E["box"], n_events=E["n_events"], seed=E["seed"],
                     yield_per_mev=E["yield_"])
     nd = g.dep_photons.size
@@ -243,10 +247,18 @@ def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wal
         se.run_events(E["box"], E["op"], E["ro"], E["tb"], E["mat"], E["yield_"], n_events=n_seg,
                       seed=E["seed"], tau_ns=E["tau"], wall_min_mm=wall_min_mm)
     e2e_s = (time.perf_counter() - t_e2e) / steps
+    # our kernels per step: per ensemble, inputs + K members x 65536-row chunks
+    # x (layer 1 + 3 tcgen05 GEMMs) + combine; then init + transport + sampler + finalize
+    chunks = lambda n: -(-int(n) // 65536)
+    launches = 2 + len(sur.members) * chunks(nd) * 4 + 4
+    for e in experts:
+        z0, z1 = e.depth_range()
+        ne = int(np.count_nonzero((g.dep_xyz[:, 2] >= z0 + se.expert_margin_mm) & (g.dep_xyz[:, 2] <= z1)))
+        launches += (2 + len(e.members) * chunks(ne) * 4) if ne else 0
     se.close()
     return dict(value=n_seg / dev_s, e2e=n_seg / e2e_s, dev_s=dev_s, mc_value=n_seg / mc_s,
                 mc_s=mc_s, mc_photon_steps=mc_steps, photons=int(off[-1]), deposits=nd,
-                members=len(sur.members),
+                members=len(sur.members), experts=len(experts), launches=launches,
                 stats=stats, photopeak_surrogate=pk_s, photopeak_mc=pk_m,
                 photopeak_shift=(pk_s["mean"] - pk_m["mean"]) / pk_m["mean"], maps=cmp,
                 h2d=int(12 * nd + 4 * nd + 8 * nd + 4 * nd), d2h=int(2 * 4 * 64 * n_seg + 4 * n_seg + 72 + 16 + nd))
@@ -604,13 +616,15 @@ def run_cuda_arm(args, W, rank, world, local_rank):
     if world == 1 and args.surrogate_events > 0 and os.path.exists(SURROGATE_BGO):
         # secondary metric: config 5, surrogate + Monte Carlo fallback vs the plain Monte Carlo
         E = surrogate_events_workload(args.surrogate_events)
-        r = run_surrogate_events_bench(eng, E, min(args.steps, 3), args.warmup, dev, stream)
+        r = run_surrogate_events_bench(eng, E, min(args.steps, 3), args.warmup, dev, stream,
+                                       expert=not args.no_expert)
         line["surrogate_events"] = {
             "metric": "511keV events/s", "workload": E["desc"], "unit": "events/s",
             "value": r["value"], "e2e": r["e2e"], "plain_mc": r["mc_value"],
             "speedup_vs_plain_mc": r["value"] / r["mc_value"],
             "photopeak_shift": r["photopeak_shift"], "maps_vs_mc": r["maps"],
-            "fallback_sites": r["stats"]["fallback_sites"], "sites": r["stats"]["sites"]}
+            "fallback_sites": r["stats"]["fallback_sites"], "sites": r["stats"]["sites"],
+            "readout_face_expert": bool(r["experts"])}
     print(json.dumps(line), flush=True)
     eng.close()
 
@@ -702,7 +716,7 @@ def run_surrogate_events_arm(args, rank, world, local_rank):
     clocks = ClockSampler(local_rank)
     clocks.start()
     r = run_surrogate_events_bench(eng, E, args.steps, args.warmup, dev, stream,
-                                   wall_min_mm=args.wall_min_mm)
+                                   wall_min_mm=args.wall_min_mm, expert=not args.no_expert)
     clk = clocks.stop()
     dev_s, e2e_s = r["dev_s"], E["n_events"] / r["e2e"]
     if world > 1:
@@ -717,12 +731,11 @@ def run_surrogate_events_arm(args, rank, world, local_rank):
                 "vs_baseline": None, "dtype": "f32+bf16", "data": "synthetic",
                 "config": {"workload": E["name"], "desc": E["desc"], "deposits": r["deposits"],
                            "photons_per_step": r["photons"], "wall_min_mm": args.wall_min_mm,
+                           "readout_face_expert": bool(r["experts"]),
                            "l2": "flushed between timed steps (256 MiB memset)"},
                 "e2e": {"value": world * E["n_events"] / e2e_s, "unit": "events/s",
                         "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
-                # per step: K members x 65536-row chunks x (layer 1 + 3 tcgen05 GEMMs),
-                # the ensemble combine, init + transport + sampler + finalize
-                "gpu_launches": args.steps * (r["members"] * -(-r["deposits"] // 65536) * 4 + 5),
+                "gpu_launches": args.steps * r["launches"],
                 "plain_mc": {"value": r["mc_value"], "unit": "events/s", "seconds": r["mc_s"],
                              "photon_steps": r["mc_photon_steps"]},
                 "speedup_vs_plain_mc": r["value"] / r["mc_value"],
@@ -758,6 +771,9 @@ def main():
     ap.add_argument("--wall-min-mm", type=float, default=1.0,
                     help="events_bgo_surrogate: sites closer than this to a wrapped face "
                          "go to the Monte Carlo")
+    ap.add_argument("--no-expert", action="store_true",
+                    help="events_bgo_surrogate: the whole-crystal ensemble only, without the "
+                         "readout-face expert")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=256,

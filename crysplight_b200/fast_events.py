@@ -51,12 +51,44 @@ class SiteLight:
     flag: object       # (n,) uint8: 1 spread, 2 near a wrapped face, 4 invalid
 
 
+class _Resident:
+    """One ensemble's networks and output scaling on the GPU."""
+
+    def __init__(self, sur: LightSurrogate, device: int, dev, max_batch: int):
+        import torch
+        self.sur = sur
+        self.nets = []
+        for p in sur.members:
+            net = MLP(device, max_batch=max_batch, seed=0)
+            net.set_params(p)
+            self.nets.append(net)
+        self.y_mean = torch.from_numpy(np.ascontiguousarray(sur.y_mean, np.float32)).to(dev)
+        self.y_std = torch.from_numpy(np.ascontiguousarray(sur.y_std, np.float32)).to(dev)
+        z0, z1 = sur.depth_range()
+        self.z0 = z0
+        # the network's input box: x, y over the crystal, depth over its slab
+        self.in_box = Box((float(sur.box_mm[0]), float(sur.box_mm[1]), z1 - z0))
+
+    def close(self):
+        for n in self.nets:
+            n.close()
+        self.nets = []
+
+
 class SurrogateEvents:
     """A ``LightSurrogate`` resident on one GPU and the surrogate event
-    generator built on it.  Not re-entrant."""
+    generator built on it.  Not re-entrant.
+
+    ``experts``: ensembles trained on a depth slab (``LightSurrogate.z_range``)
+    of the same crystal, e.g. the last millimetres before the readout face,
+    where the light of a site concentrates under one SiPM and one network for
+    the whole crystal is least certain.  A site deeper than an expert's slab
+    start plus ``expert_margin_mm`` takes that expert's outputs (spread and
+    flags included) instead of the main ensemble's; the margin keeps the
+    slab's edge, where its training data ends, out of use."""
 
     def __init__(self, surrogate: LightSurrogate, engine=None, device: int = 0,
-                 max_batch: int = 65536):
+                 max_batch: int = 65536, experts=(), expert_margin_mm: float = 1.0):
         import torch
         from .transport import Engine
         self.sur = surrogate
@@ -64,36 +96,44 @@ class SurrogateEvents:
         self.dev = torch.device("cuda", device)
         self.engine = engine or Engine(device)
         self.lib = _lib.load()
-        self.nets = []
-        for p in surrogate.members:
-            net = MLP(device, max_batch=max_batch, seed=0)
-            net.set_params(p)
-            self.nets.append(net)
-        self.y_mean = torch.from_numpy(np.ascontiguousarray(surrogate.y_mean, np.float32)).to(self.dev)
-        self.y_std = torch.from_numpy(np.ascontiguousarray(surrogate.y_std, np.float32)).to(self.dev)
         self.box = Box(tuple(float(v) for v in surrogate.box_mm))
+        self.main = _Resident(surrogate, device, self.dev, max_batch)
+        self.experts = []
+        for e in experts:
+            if tuple(float(v) for v in e.box_mm) != tuple(float(v) for v in surrogate.box_mm):
+                raise ValueError("an expert was trained for another crystal size")
+            if e.z_range is None:
+                raise ValueError("an expert needs a depth range (LightSurrogate.z_range)")
+            self.experts.append(_Resident(e, device, self.dev, max_batch))
+        self.expert_margin_mm = float(expert_margin_mm)
+
+    @property
+    def nets(self):
+        return self.main.nets
 
     def close(self):
-        for n in self.nets:
-            n.close()
-        self.nets = []
+        for r in [self.main] + self.experts:
+            r.close()
 
-    def site_light(self, xyz, *, ro: Readout, pde: float, spread_max: float = SPREAD_MAX,
-                   wall_min_mm: float = WALL_MIN_MM, stream=None) -> SiteLight:
-        """Ensemble outputs for sites xyz ((n, 3) float32 CUDA tensor, mm)."""
+    def _light(self, ens: _Resident, xyz, ro: Readout, pde: float, spread_max: float,
+               wall_min_mm: float, stream) -> SiteLight:
+        """One ensemble on sites xyz ((n, 3) float32 CUDA tensor, mm)."""
         import torch
         n = int(xyz.shape[0])
-        K = len(self.nets)
+        K = len(ens.nets)
         xyz = xyz.contiguous()
         xin = torch.empty((n, 3), dtype=torch.float32, device=self.dev)
-        rc = self.lib.cl_surrogate_inputs(C.c_void_p(xyz.data_ptr()), n, C.byref(self.box),
-                                          float(self.sur.z_warp), C.c_void_p(xin.data_ptr()),
+        xs = xyz
+        if ens.z0 != 0.0:
+            xs = xyz - torch.tensor([0.0, 0.0, ens.z0], dtype=torch.float32, device=self.dev)
+        rc = self.lib.cl_surrogate_inputs(C.c_void_p(xs.data_ptr()), n, C.byref(ens.in_box),
+                                          float(ens.sur.z_warp), C.c_void_p(xin.data_ptr()),
                                           stream_arg(stream))
         if rc != 0:
             raise _lib.CudaTransportError(rc, "cl_surrogate_inputs failed")
         torch.cuda.synchronize(self.dev)         # the networks run on their own streams
         raw = torch.empty((K, n, D_OUT), dtype=torch.float32, device=self.dev)
-        for k, net in enumerate(self.nets):
+        for k, net in enumerate(ens.nets):
             if n:
                 net.forward_into(xin, raw[k])
         out = SiteLight(torch.empty((n, N_CELLS), dtype=torch.float32, device=self.dev),
@@ -103,12 +143,32 @@ class SurrogateEvents:
                         torch.empty(n, dtype=torch.uint8, device=self.dev))
         P = C.c_void_p
         rc = self.lib.cl_surrogate_combine(
-            P(raw.data_ptr()), K, n, P(self.y_mean.data_ptr()), P(self.y_std.data_ptr()),
+            P(raw.data_ptr()), K, n, P(ens.y_mean.data_ptr()), P(ens.y_std.data_ptr()),
             P(xyz.data_ptr()), C.byref(self.box), C.byref(ro), float(pde), float(spread_max),
             float(wall_min_mm), P(out.p.data_ptr()), P(out.tmean.data_ptr()), P(out.tsig.data_ptr()),
             P(out.spread.data_ptr()), P(out.flag.data_ptr()), stream_arg(stream))
         if rc != 0:
             raise _lib.CudaTransportError(rc, "cl_surrogate_combine failed")
+        return out
+
+    def site_light(self, xyz, *, ro: Readout, pde: float, spread_max: float = SPREAD_MAX,
+                   wall_min_mm: float = WALL_MIN_MM, stream=None) -> SiteLight:
+        """Ensemble outputs for sites xyz ((n, 3) float32 CUDA tensor, mm),
+        each site from the main ensemble or the expert whose slab holds it."""
+        import torch
+        out = self._light(self.main, xyz, ro, pde, spread_max, wall_min_mm, stream)
+        for ens in self.experts:
+            z0, z1 = ens.sur.depth_range()
+            z = xyz[:, 2]
+            idx = torch.nonzero((z >= z0 + self.expert_margin_mm) & (z <= z1)).flatten()
+            if idx.numel() == 0:
+                continue
+            sub = self._light(ens, xyz.index_select(0, idx), ro, pde, spread_max, wall_min_mm, stream)
+            torch.cuda.synchronize(self.dev)     # both combines ran on `stream`
+            for name in ("p", "tmean", "tsig", "spread", "flag"):
+                getattr(out, name).index_copy_(0, idx, getattr(sub, name))
+        if self.experts:
+            torch.cuda.synchronize(self.dev)
         return out
 
     def transport_sites(self, box: Box, op: OpticalParams, ro: Readout, tb: TimeBinning, *,

@@ -163,16 +163,18 @@ def depth_unwarp(w, a: float):
     return 0.5 * (lo + hi)
 
 
-def grid_points(box: Box, shape=(48, 48, 24), z_warp: float = 0.0) -> np.ndarray:
+def grid_points(box: Box, shape=(48, 48, 24), z_warp: float = 0.0, z_range=None) -> np.ndarray:
     """Cell centres of a regular nx x ny x nz grid over the crystal, (P, 3)
     float32 in mm, x fastest; with ``z_warp`` the z levels are the cell
     centres of a regular grid in the warped depth (denser towards the readout
-    face)."""
+    face); ``z_range`` = (z0, z1) mm restricts the grid to that slab."""
     nx, ny, nz = shape
     L = [float(box.L[i]) for i in range(3)]
-    ax = [(np.arange(n, dtype=np.float64) + 0.5) * (L[i] / n) for i, n in enumerate((nx, ny, nz))]
+    z0, z1 = (0.0, L[2]) if z_range is None else (float(z_range[0]), float(z_range[1]))
+    ax = [(np.arange(n, dtype=np.float64) + 0.5) * (L[i] / n) for i, n in enumerate((nx, ny))]
+    ax.append(z0 + (np.arange(nz, dtype=np.float64) + 0.5) * ((z1 - z0) / nz))
     if z_warp:
-        ax[2] = depth_unwarp((np.arange(nz, dtype=np.float64) + 0.5) / nz, z_warp) * L[2]
+        ax[2] = z0 + depth_unwarp((np.arange(nz, dtype=np.float64) + 0.5) / nz, z_warp) * (z1 - z0)
     z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
     return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1).astype(np.float32)
 
@@ -286,22 +288,30 @@ class LightSurrogate:
     members: list               # K parameter vectors (float32)
     cells: int = N_CELLS
     meta: dict = field(default_factory=dict)
-    z_warp: float = 0.0         # network input depth: 2 depth_warp(z / Lz) - 1
+    z_warp: float = 0.0         # network input depth: 2 depth_warp((z - z0) / (z1 - z0)) - 1
+    z_range: Optional[tuple] = None   # (z0, z1) mm of a slab ensemble; None: the whole crystal
+
+    def depth_range(self) -> tuple:
+        """(z0, z1) in mm: the depths the network's input spans."""
+        if self.z_range is None:
+            return 0.0, float(self.box_mm[2])
+        return float(self.z_range[0]), float(self.z_range[1])
 
     def normalise(self, xyz: np.ndarray) -> np.ndarray:
-        """Network inputs: x and y scaled to [-1, 1], z through the depth warp."""
+        """Network inputs: x and y scaled to [-1, 1]; z through the depth warp
+        of its position in the ensemble's depth range (clamped to it)."""
         q = np.asarray(xyz, np.float64).reshape(-1, 3)
         L = self.box_mm.astype(np.float64)
         out = 2.0 * q / L - 1.0
-        if self.z_warp:
-            out[:, 2] = 2.0 * depth_warp(q[:, 2] / L[2], self.z_warp) - 1.0
+        z0, z1 = self.depth_range()
+        out[:, 2] = 2.0 * depth_warp((q[:, 2] - z0) / (z1 - z0), self.z_warp) - 1.0
         return out.astype(np.float32)
 
     @classmethod
     def train(cls, box: Box, xyz: np.ndarray, targets: np.ndarray, *, members: int = 5, steps: int = 20000,
               batch: int = 65536, lr: float = 1e-3, lr_final: Optional[float] = None,
-              time_weight: float = 1.0, z_warp: float = 0.0, seed: int = 0, device: int = 0,
-              chunk: int = 250, log=None):
+              time_weight: float = 1.0, z_warp: float = 0.0, z_range=None, seed: int = 0,
+              device: int = 0, chunk: int = 250, log=None):
         """Train ``members`` networks on standardised targets.
 
         ``lr_final``: cosine decay of the Adam step size from ``lr`` to
@@ -316,7 +326,8 @@ class LightSurrogate:
         y_mean = targets.mean(0).astype(np.float64)
         y_std = np.maximum(targets.std(0), 1e-6).astype(np.float64)
         y_std[N_CELLS:] /= math.sqrt(time_weight)
-        obj = cls(L, y_mean.astype(np.float32), y_std.astype(np.float32), [], z_warp=float(z_warp))
+        obj = cls(L, y_mean.astype(np.float32), y_std.astype(np.float32), [], z_warp=float(z_warp),
+                  z_range=None if z_range is None else (float(z_range[0]), float(z_range[1])))
         x = torch.from_numpy(obj.normalise(xyz)).to(f"cuda:{device}")
         y = torch.from_numpy(((targets - y_mean) / y_std).astype(np.float32)).to(f"cuda:{device}")
         history = []
@@ -339,7 +350,7 @@ class LightSurrogate:
             history.append(hist)
             net.close()
         obj.meta = {"steps": steps, "batch": batch, "lr": lr, "lr_final": lr_final,
-                    "time_weight": time_weight, "z_warp": z_warp, "seed": seed,
+                    "time_weight": time_weight, "z_warp": z_warp, "z_range": obj.z_range, "seed": seed,
                     "train_seconds": time.perf_counter() - t0, "loss_history": history}
         return obj
 
@@ -372,10 +383,14 @@ class LightSurrogate:
     def save(self, path: str):
         np.savez_compressed(path, box_mm=self.box_mm, y_mean=self.y_mean, y_std=self.y_std,
                             members=np.stack(self.members), cells=self.cells, z_warp=np.float64(self.z_warp),
+                            z_range=np.float64(self.depth_range() if self.z_range is not None else (np.nan, np.nan)),
                             meta=np.array(repr({k: v for k, v in self.meta.items() if k != "loss_history"})))
 
     @classmethod
     def load(cls, path: str):
         z = np.load(path, allow_pickle=False)
+        zr = None
+        if "z_range" in z.files and np.all(np.isfinite(z["z_range"])):
+            zr = (float(z["z_range"][0]), float(z["z_range"][1]))
         return cls(z["box_mm"], z["y_mean"], z["y_std"], list(z["members"]), int(z["cells"]),
-                   {"saved": str(z["meta"])}, float(z["z_warp"]) if "z_warp" in z.files else 0.0)
+                   {"saved": str(z["meta"])}, float(z["z_warp"]) if "z_warp" in z.files else 0.0, zr)

@@ -102,6 +102,12 @@ def main(argv=None):
                     help="cosine decay of the step size to this value (negative: constant lr)")
     ap.add_argument("--z-warp", type=float, default=0.0,
                     help="depth warp of the grid and of the network input (0 = uniform in z)")
+    ap.add_argument("--z-range", type=float, nargs=2, default=None, metavar=("Z0", "Z1"),
+                    help="train an expert for the depth slab z0..z1 mm (grid and network input "
+                         "span the slab; the event generator uses it for sites inside)")
+    ap.add_argument("--compare-model", default=None,
+                    help="also validate this ensemble (.npz, e.g. the whole-crystal one) on the "
+                         "same held-out points")
     ap.add_argument("--time-weight", type=float, default=0.1,
                     help="loss weight of the arrival-time outputs relative to the probabilities")
     ap.add_argument("--seed", type=int, default=4242)
@@ -121,8 +127,9 @@ def main(argv=None):
     eng = Engine(args.device)
     rep = {"setup": args.setup, "grid": list(args.grid), "photons_per_point": args.photons,
            "members": args.members, "steps": args.steps, "batch": args.batch, "lr": args.lr,
-           "lr_final": args.lr_final, "time_weight": args.time_weight, "z_warp": args.z_warp}
-    pts = grid_points(box, tuple(args.grid), z_warp=args.z_warp)
+           "lr_final": args.lr_final, "time_weight": args.time_weight, "z_warp": args.z_warp,
+           "z_range": args.z_range}
+    pts = grid_points(box, tuple(args.grid), z_warp=args.z_warp, z_range=args.z_range)
     scan = scan_light(eng, box, op, ro, points=pts, photons_per_point=args.photons, seed=args.seed)
     n_ph = pts.shape[0] * args.photons
     rep["scan"] = {"points": int(pts.shape[0]), "photons": n_ph, "seconds": scan.seconds,
@@ -137,7 +144,8 @@ def main(argv=None):
         sur = LightSurrogate.train(box, pts[tr], y[tr], members=args.members, steps=args.steps,
                                    batch=args.batch, lr=args.lr,
                                    lr_final=args.lr_final if args.lr_final >= 0 else None,
-                                   time_weight=args.time_weight, z_warp=args.z_warp, seed=args.seed,
+                                   time_weight=args.time_weight, z_warp=args.z_warp,
+                                   z_range=args.z_range, seed=args.seed,
                                    device=args.device,
                                    log=lambda s: print(s, flush=True))
         rep["train_seconds"] = sur.meta["train_seconds"]
@@ -183,6 +191,25 @@ def main(argv=None):
     rep["holdout"]["by_distance_to_readout_mm"] = {
         f"{lo}-{hi}": float(per_pt[(dz_read >= lo) & (dz_read < hi)].mean())
         for lo, hi in ((0, 2), (2, 5), (5, 10), (10, 30)) if ((dz_read >= lo) & (dz_read < hi)).any()}
+    bins_read = ((0, 1), (1, 2), (2, 4), (4, 8), (8, 30))
+    rep["holdout"]["spread_above_2pct_by_distance_to_readout_mm"] = {
+        f"{lo}-{hi}": float(np.mean(pred["spread"][(dz_read >= lo) & (dz_read < hi)] > 0.02))
+        for lo, hi in bins_read if ((dz_read >= lo) & (dz_read < hi)).any()}
+    if args.compare_model:
+        other = LightSurrogate.load(args.compare_model).predict(pts[sub], device=args.device)
+        per_o = np.array([rel_error(other["p"][i:i + 1], p_true[i:i + 1], args.photons)["mean"]
+                          for i in range(sub.size)])
+        rep["holdout"]["compare_model"] = {
+            "path": args.compare_model, "surrogate": rel_error(other["p"], p_true, args.photons),
+            "by_distance_to_readout_mm": {
+                f"{lo}-{hi}": float(per_o[(dz_read >= lo) & (dz_read < hi)].mean())
+                for lo, hi in bins_read if ((dz_read >= lo) & (dz_read < hi)).any()},
+            "spread_above_2pct_by_distance_to_readout_mm": {
+                f"{lo}-{hi}": float(np.mean(other["spread"][(dz_read >= lo) & (dz_read < hi)] > 0.02))
+                for lo, hi in bins_read if ((dz_read >= lo) & (dz_read < hi)).any()}}
+        rep["holdout"]["surrogate_by_distance_to_readout_mm_fine"] = {
+            f"{lo}-{hi}": float(per_pt[(dz_read >= lo) & (dz_read < hi)].mean())
+            for lo, hi in bins_read if ((dz_read >= lo) & (dz_read < hi)).any()}
     rep["holdout"]["by_distance_to_wall_mm"] = {
         f"{lo}-{hi}": float(per_pt[(d_wall >= lo) & (d_wall < hi)].mean())
         for lo, hi in ((0, 1), (1, 3), (3, 8), (8, 30)) if ((d_wall >= lo) & (d_wall < hi)).any()}
@@ -193,7 +220,8 @@ def main(argv=None):
                 json.dump(rep, f, indent=1)
         eng.close()
         return rep
-    sur.meta.update({"setup": args.setup, "grid": list(args.grid), "photons_per_point": args.photons})
+    sur.meta.update({"setup": args.setup, "grid": list(args.grid), "photons_per_point": args.photons,
+                     "z_range": args.z_range})
     sur.save(args.out)
     if args.report:
         with open(args.report, "w") as f:

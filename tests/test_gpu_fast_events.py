@@ -211,3 +211,54 @@ def test_sampling_reproduces_the_monte_carlo(engine):
             b = m_tmin[sl][both[:, c], c]
             se = np.sqrt(a.var() / a.size + b.var() / b.size)
             assert abs(a.mean() - b.mean()) < 5 * se + 0.5, (k, c, a.mean(), b.mean(), se)
+
+
+def test_depth_slab_expert_serves_the_sites_inside_its_slab(engine):
+    """An expert ensemble replaces the main one exactly for the sites deeper
+    than its slab start plus the margin; the other sites keep the main
+    ensemble's outputs, and an expert spanning the whole crystal with the
+    same networks changes nothing."""
+    import os
+    import torch
+    from crysplight_b200.fast_events import SurrogateEvents
+    from crysplight_b200.surrogate import LightSurrogate
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    main = LightSurrogate.load(os.path.join(root, "crysplight_b200", "surrogates", "bgo_esr.npz"))
+    L = [float(v) for v in main.box_mm]
+    rng = np.random.default_rng(4)
+    xyz = np.stack([rng.uniform(0.5, L[0] - 0.5, 3000), rng.uniform(0.5, L[1] - 0.5, 3000),
+                    rng.uniform(0.0, L[2], 3000)], 1).astype(np.float32)
+    d = torch.from_numpy(xyz).cuda()
+    from crysplight_b200.params import Readout, SipmGrid
+    ro = Readout(SipmGrid(6.0, 8, 8))
+    kw = dict(ro=ro, pde=0.4)
+
+    def light(se):
+        s = se.site_light(d, **kw)
+        return {k: getattr(s, k).cpu().numpy() for k in ("p", "tmean", "tsig", "spread", "flag")}
+
+    se0 = SurrogateEvents(main, engine)
+    ref = light(se0)
+    se0.close()
+    whole = LightSurrogate(main.box_mm, main.y_mean, main.y_std, main.members, z_range=(0.0, L[2]))
+    se1 = SurrogateEvents(main, engine, experts=[whole], expert_margin_mm=1.0)
+    same = light(se1)
+    se1.close()
+    for k in ref:
+        assert np.array_equal(ref[k], same[k]), k
+    # a slab over the readout half: its own input mapping, so other outputs
+    z0 = 0.5 * L[2]
+    slab = LightSurrogate(main.box_mm, main.y_mean, main.y_std, main.members[:3], z_range=(z0, L[2]))
+    se2 = SurrogateEvents(main, engine, experts=[slab], expert_margin_mm=1.0)
+    mixed = light(se2)
+    se2.close()
+    inside = xyz[:, 2] >= z0 + 1.0
+    se3 = SurrogateEvents(slab, engine)      # the slab ensemble alone, on the inside sites
+    sub = se3.site_light(d[torch.from_numpy(np.nonzero(inside)[0]).cuda()], **kw)
+    own = {k: getattr(sub, k).cpu().numpy() for k in ref}
+    se3.close()
+    assert 0 < inside.sum() < inside.size
+    for k in ref:
+        assert np.array_equal(mixed[k][~inside], ref[k][~inside]), k
+        assert np.array_equal(mixed[k][inside], own[k]), k
+    assert not np.array_equal(mixed["p"][inside], ref["p"][inside])

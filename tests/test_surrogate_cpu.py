@@ -35,6 +35,28 @@ def test_inputs_and_depth_warp():
     assert z == pytest.approx(2 * depth_warp(0.5, 0.5) - 1, abs=1e-6)
 
 
+def test_depth_slab_inputs_grid_and_persistence(tmp_path):
+    """An expert for the slab z0..z1: its grid lies in the slab, its network
+    input maps the slab onto [-1, 1] (clamped outside), and the range survives
+    save/load (the whole-crystal ensembles keep z_range None)."""
+    box = Box((48.0, 48.0, 22.4))
+    g = grid_points(box, (2, 2, 4), z_range=(14.4, 22.4))
+    assert np.allclose(np.unique(g[:, 2]), [15.4, 17.4, 19.4, 21.4])
+    s = LightSurrogate(np.array([48.0, 48.0, 22.4]), np.zeros(192), np.ones(192),
+                       [np.zeros(4, np.float32)], z_range=(14.4, 22.4))
+    assert s.depth_range() == (14.4, 22.4)
+    x = s.normalise([[0.0, 48.0, 14.4], [24.0, 24.0, 22.4], [24.0, 24.0, 18.4], [1.0, 1.0, 3.0]])
+    assert np.allclose(x[:, 2], [-1.0, 1.0, 0.0, -1.0], atol=1e-6)
+    assert np.allclose(x[:, :2], [[-1, 1], [0, 0], [0, 0], [2 / 48 - 1, 2 / 48 - 1]])
+    p = str(tmp_path / "slab.npz")
+    s.save(p)
+    assert LightSurrogate.load(p).z_range == (14.4, 22.4)
+    w = LightSurrogate(np.array([48.0, 48.0, 22.4]), np.zeros(192), np.ones(192), [np.zeros(4, np.float32)])
+    w.save(p)
+    t = LightSurrogate.load(p)
+    assert t.z_range is None and t.depth_range() == (0.0, 22.4)
+
+
 def test_grid_and_holdout():
     box = Box((48.0, 48.0, 22.4))
     g = grid_points(box, (4, 3, 2))
