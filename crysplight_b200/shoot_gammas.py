@@ -141,6 +141,9 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("configs", nargs="+")
     ap.add_argument("--surrogate", default=None, help="trained LightSurrogate (.npz)")
+    ap.add_argument("--expert", action="append", default=[],
+                    help="depth-slab expert ensemble (.npz) used with --surrogate for the sites "
+                         "inside its slab (repeatable)")
     ap.add_argument("--n-events", type=int, default=None, help="override the run file's n_events")
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args(argv)
@@ -150,7 +153,8 @@ def main(argv=None):
     if args.surrogate:
         from .fast_events import SurrogateEvents
         from .surrogate import LightSurrogate
-        se = SurrogateEvents(LightSurrogate.load(args.surrogate), eng, device=args.device)
+        se = SurrogateEvents(LightSurrogate.load(args.surrogate), eng, device=args.device,
+                             experts=[LightSurrogate.load(p) for p in args.expert])
     for path in args.configs:
         shoot_gammas(path, engine=eng, surrogate=se, n_events=args.n_events)
     if se is not None:
