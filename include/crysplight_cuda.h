@@ -417,7 +417,7 @@ int cl_mlp_gradient(cl_mlp* m, const float* d_x, const float* d_t, int B, float*
 
 /* ---------------------------------------------------------------------------
  * Host-side 511 keV gamma stage of the event pipeline (no GPU involved).
- * The reference runs it in Julia (its vendored gamma core, src/gamma/*.jl,
+ * The reference runs it in Julia (its vendored gamma core, the src/gamma files,
  * through src/gamma_interface.jl); these restate it in C.  Each event draws
  * from its own Philox4x32-10 stream keyed by (seed, event number), so the
  * gamma stage is statistically, not bitwise, equivalent to the reference
