@@ -59,6 +59,10 @@ L2_FLUSH_BYTES = 256 << 20
 # sources, offsets and maps are 0.24 MB.  point1m: not captured.
 TRAFFIC_PER_STEP = (3.003459e9 + 6.809856e6) / 494_804_727
 TRAFFIC_BYTES = {"point1m": None}
+# Warp instructions the transport kernel issues per photon-step (smsp__inst_executed
+# of the same ncu capture: 17.46 G for 494.8M photon-steps); with the live
+# steps/s this gives the kernel's issue rate against the SMs' issue slots.
+WARP_INST_PER_STEP = {"scan256": 17458537737 / 494_804_727}
 
 
 def events_workload(n_events: int = 50_000):
@@ -284,6 +288,20 @@ def events_cpu_baseline(E, target_s: float) -> dict:
     return {"value": n / dt, "unit": "events/s", "cores": os.cpu_count(), "kind": "port",
             "sample": f"first {n} of the {E['n_events']} events ({dt:.1f} s on "
                       f"{os.cpu_count()} threads; gamma stage excluded)"}
+
+
+def issue_slots(name: str, steps_per_s: float, n_sm: int, sm_mhz: float):
+    """The transport kernel's warp-instruction issue rate (warp instructions
+    per photon-step from the committed ncu capture x the live photon-steps/s)
+    against the SMs' issue slots (4 schedulers per SM, one instruction per
+    clock each, at the max SM clock); None where no capture exists."""
+    wi = WARP_INST_PER_STEP.get(name)
+    if wi is None:
+        return None
+    achieved = wi * steps_per_s
+    peak = n_sm * 4 * sm_mhz * 1e6
+    return {"achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "G warp-instructions/s",
+            "frac": achieved / peak, "warp_inst_per_step": wi}
 
 
 def workload(name: str, points: int = 256, per_point: int = 200_000):
@@ -596,6 +614,8 @@ def run_cuda_arm(args, W, rank, world, local_rank):
                      "one op per lane per clock (SMs x 128 lanes x max SM clock of measured)"),
             "hbm": {"achieved": out_bytes / launch_s / 1e9, "peak": peaks.get("hbm_gbs"),
                     "unit": "GB/s", "frac": out_bytes / launch_s / 1e9 / peaks.get("hbm_gbs", 1)},
+            "issue_slots": issue_slots(W["name"], steps_per_launch / launch_s, n_sm,
+                                       peaks.get("sm_max_mhz", 1965.0)),
         },
         "clocks": clk,
         "wall_s_timed": t_wall,
