@@ -53,16 +53,16 @@ OPS_PER_STEP = {"scan256": 165.6, "point1m": 186.7}
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per launch of the transport kernel: one ncu capture
 # of the scan at 20,000 photons per point (profiles/transport_kernel_scan256x20k.md,
-# 3.01 GB for 494.8M photon-steps) scaled to the full launch by photon-steps.
+# 3.00 GB for 494.8M photon-steps) scaled to the full launch by photon-steps.
 # Almost all of it is L2 misses of the 64 MB log table (about 2 bytes per
 # photon-step x log lookup), which grow in proportion to the steps; the
 # sources, offsets and maps are 0.24 MB.  point1m: not captured.
-TRAFFIC_PER_STEP = (3.003459e9 + 6.809856e6) / 494_804_727
+TRAFFIC_PER_STEP = (2.993991e9 + 6.48064e6) / 494_804_727
 TRAFFIC_BYTES = {"point1m": None}
 # Warp instructions the transport kernel issues per photon-step (smsp__inst_executed
-# of the same ncu capture: 17.46 G for 494.8M photon-steps); with the live
+# of the same ncu capture: 17.23 G for 494.8M photon-steps); with the live
 # steps/s this gives the kernel's issue rate against the SMs' issue slots.
-WARP_INST_PER_STEP = {"scan256": 17458537737 / 494_804_727}
+WARP_INST_PER_STEP = {"scan256": 17228482017 / 494_804_727}
 
 
 def events_workload(n_events: int = 50_000):
