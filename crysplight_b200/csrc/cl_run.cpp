@@ -375,10 +375,22 @@ int main(int argc, char** argv)
             if (i + 1 >= argc) { std::fprintf(stderr, "%s needs a value\n", name); std::exit(2); }
             return argv[++i];
         };
-        if (a == "--device") device = std::atoi(arg("--device").c_str());
+        // a non-negative decimal integer, or exit 2
+        auto count = [&](const char* name) -> long long {
+            const std::string v = arg(name);
+            char* end = nullptr;
+            errno = 0;
+            const long long x = std::strtoll(v.c_str(), &end, 10);
+            if (v.empty() || *end != 0 || errno != 0 || x < 0) {
+                std::fprintf(stderr, "%s needs a non-negative integer, got '%s'\n", name, v.c_str());
+                std::exit(2);
+            }
+            return x;
+        };
+        if (a == "--device") device = (int)count("--device");
         else if (a == "--data") data_dir = arg("--data");
         else if (a == "--output-root") out_root = arg("--output-root");
-        else if (a == "--n-photons") n_override = std::atoll(arg("--n-photons").c_str());
+        else if (a == "--n-photons") n_override = count("--n-photons");
         else if (a == "--print-setup") print_only = true;
         else if (a == "--no-write") write = false;
         else if (a == "-h" || a == "--help") { usage(); return 0; }

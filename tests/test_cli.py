@@ -122,6 +122,18 @@ def test_toml_errors_name_the_line(cli, tmp_path, bad, msg):
     assert r.returncode == 1 and msg in r.stderr and "bad.toml:" in r.stderr, r.stderr
 
 
+@pytest.mark.parametrize("args", [["--n-photons", "12x"], ["--n-photons", "-5"], ["--device", ""],
+                                  ["--bogus"], []])
+def test_bad_command_lines_exit_2(cli, args):
+    r = subprocess.run([cli, *args, "--print-setup", RUNS[0]] if args else [cli], capture_output=True,
+                       text=True)
+    assert r.returncode == 2, (args, r.stderr)
+
+
+def test_n_photons_override(cli):
+    assert _setup_json(cli, RUNS[0], "--n-photons", "1234")["n_photons"] == 1234
+
+
 def test_missing_material_and_unknown_finish_are_errors(cli, tmp_path):
     txt = open(RUNS[0]).read()
     p = tmp_path / "m.toml"
