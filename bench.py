@@ -66,7 +66,7 @@ WARP_INST_PER_STEP = {"scan256": 17228482017 / 494_804_727}
 
 
 def events_workload(n_events: int = 50_000):
-    """Config 3: 511 keV gammas on CsI(Tl) + Teflon (runs/gammas_csitl_50k.toml:
+    """511 keV gammas on CsI(Tl) + Teflon (runs/gammas_csitl_50k.toml:
     seed 11, PDE 0.40, 100 ns x 80 bins, yield 54000/MeV, tau 1000 ns)."""
     from crysplight_b200.params import (Box, OpticalParams, Readout, SipmGrid, TimeBinning,
                                         deg2rad_f32)
@@ -161,7 +161,7 @@ SURROGATE_BGO_FACE = os.path.join(ROOT, "crysplight_b200", "surrogates", "bgo_es
 
 
 def surrogate_events_workload(n_events: int = 500_000):
-    """Config 5: 511 keV gammas on BGO + ESR (geometry of runs/gammas_bgo_500k.toml,
+    """511 keV gammas on BGO + ESR (geometry of runs/gammas_bgo_500k.toml,
     48x48x22.4 mm, PDE 0.40, 100 ns x 120 bins; seed 99, yield 14000/MeV,
     tau 1768 ns, density 7.13 g/cm3)."""
     from crysplight_b200.params import (Box, OpticalParams, Readout, SipmGrid, TimeBinning,
@@ -623,7 +623,7 @@ def run_cuda_arm(args, W, rank, world, local_rank):
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(W, args.cpu_seconds)
     if world == 1 and args.events > 0:
-        # secondary metric: 511 keV events/s of the event pipeline (config 3 sample)
+        # secondary metric: 511 keV events/s of the event pipeline (10,000 CsI(Tl) events)
         E = events_workload(args.events)
         r = run_events_bench(eng, E, args.steps, args.warmup, dev, stream)
         line["events"] = {"metric": "511keV events/s", "workload": E["desc"],
@@ -634,7 +634,8 @@ def run_cuda_arm(args, W, rank, world, local_rank):
     if world == 1 and args.surrogate_training:
         line["surrogate_training"] = surrogate_training_bench(dev)
     if world == 1 and args.surrogate_events > 0 and os.path.exists(SURROGATE_BGO):
-        # secondary metric: config 5, surrogate + Monte Carlo fallback vs the plain Monte Carlo
+        # secondary metric: 500,000 BGO+ESR events, surrogate + Monte Carlo fallback vs
+        # the plain Monte Carlo
         E = surrogate_events_workload(args.surrogate_events)
         r = run_surrogate_events_bench(eng, E, min(args.steps, 3), args.warmup, dev, stream,
                                        expert=not args.no_expert)
@@ -710,7 +711,7 @@ def run_events_arm(args, rank, world, local_rank):
 
 def run_surrogate_events_arm(args, rank, world, local_rank):
     """--workload events_bgo_surrogate: events/s of the surrogate + Monte Carlo
-    fallback pipeline (config 5), the plain CUDA Monte Carlo on the same events,
+    fallback pipeline (500,000 BGO+ESR events), the plain CUDA Monte Carlo on the same events,
     and their agreement (photopeak, per-SiPM chi2)."""
     import torch
     import crysplight_b200 as cl

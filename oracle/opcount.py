@@ -67,6 +67,6 @@ if __name__ == "__main__":
                              pos=tuple(pts[pidx]), pid_offset=pidx * 200_000, tau_ns=1768.0)
         tot_ops += o * sp * 20_000
         tot_steps += sp * 20_000
-    print(f"config1 (CsI(Tl)+Teflon centre): {r1[0]:.1f} ops/step, {r1[1]:.2f} steps/photon")
-    print(f"config2 (BGO+ESR 16 of 256 scan points): {tot_ops / tot_steps:.1f} ops/step, "
+    print(f"CsI(Tl)+Teflon point source (centre): {r1[0]:.1f} ops/step, {r1[1]:.2f} steps/photon")
+    print(f"BGO+ESR scan (16 of 256 points): {tot_ops / tot_steps:.1f} ops/step, "
           f"{tot_steps / (16 * 20_000):.2f} steps/photon")

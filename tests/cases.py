@@ -24,12 +24,12 @@ def ideal(n_crystal, *, wrap_R=1.0, spec=False, abs_len=INF, ray=INF, gap=True, 
     return OpticalParams(n_crystal, 1.45, abs_len, ray, wrap_R, spec, gap, sigma, pde)
 
 
-# Config 1: CsI(Tl) + Teflon, PDE 1 (runs/point_csitl_teflon.toml + data/*.toml)
-OP_C1 = OpticalParams(1.79, 1.45, 3115.0, 346.0, 0.99, False, True, deg2rad_f32(1.3), 1.0)
-TAU_C1 = 1000.0
-# Config 2: BGO + ESR, PDE 1 (runs/point_bgo_esr.toml + data/bgo.toml, data/esr.toml)
-OP_C2 = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, deg2rad_f32(1.3), 1.0)
-TAU_C2 = 1768.0
+# CsI(Tl) + Teflon, PDE 1 (runs/point_csitl_teflon.toml + data/*.toml)
+OP_CSI_TEFLON = OpticalParams(1.79, 1.45, 3115.0, 346.0, 0.99, False, True, deg2rad_f32(1.3), 1.0)
+TAU_CSI = 1000.0
+# BGO + ESR, PDE 1 (runs/point_bgo_esr.toml + data/bgo.toml, data/esr.toml)
+OP_BGO_ESR = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, deg2rad_f32(1.3), 1.0)
+TAU_BGO = 1768.0
 # every process at once (test/runtests.jl:168-170, 229-231)
 OP_ALL = OpticalParams(1.95, 1.45, 500.0, 400.0, 0.98, False, True, deg2rad_f32(6.0), 0.4)
 RO_ALL = Readout(GRID, center=(24, 24), radius=20, sur_R=0.9)

@@ -4,7 +4,7 @@ autotuner picks one of its candidates."""
 import numpy as np
 import pytest
 
-from cases import BOX_CSI, GRID, OP_C1, TB80
+from cases import BOX_CSI, GRID, OP_CSI_TEFLON, TB80
 
 pytestmark = pytest.mark.gpu
 
@@ -21,7 +21,7 @@ def _device_events(engine, g):
     import torch
     from crysplight_b200.batching import DeviceEvents
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
-    return DeviceEvents(engine, BOX_CSI, OP_C1, GRID, TB80, xyz=T(g.dep_xyz), t0=T(g.dep_t),
+    return DeviceEvents(engine, BOX_CSI, OP_CSI_TEFLON, GRID, TB80, xyz=T(g.dep_xyz), t0=T(g.dep_t),
                         photons=T(g.dep_photons), segment=T(g.dep_event), n_segments=1500, seed=8,
                         tau_ns=1000.0)
 
@@ -35,7 +35,7 @@ def _same(a, b):
 
 def test_graph_replay_equals_the_host_call(engine, deposits):
     g = deposits
-    ref = engine.run_segments(BOX_CSI, OP_C1, GRID, TB80, sources=g.dep_xyz, photons_per_source=g.dep_photons,
+    ref = engine.run_segments(BOX_CSI, OP_CSI_TEFLON, GRID, TB80, sources=g.dep_xyz, photons_per_source=g.dep_photons,
                               segment_of_source=g.dep_event, n_segments=1500, seed=8, t0s=g.dep_t,
                               tau_ns=1000.0)
     ev = _device_events(engine, g)

@@ -6,7 +6,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from cases import BOX_BGO, GRID, OP_C2, TB80
+from cases import BOX_BGO, GRID, OP_BGO_ESR, TB80
 
 pytestmark = pytest.mark.gpu
 
@@ -22,7 +22,7 @@ def test_events_surrogate_rejects_bad_arguments(engine):
         a = dict(n_src=0, n_photons=0, n_sites=0, n_segments=1, maps=1, tmin=1, npe=1, ctr=1, sx=None)
         a.update(over)
         return lib.cl_run_events_surrogate_device(
-            engine.handle, C.byref(BOX_BGO), C.byref(OP_C2), C.byref(ro), C.byref(TB80),
+            engine.handle, C.byref(BOX_BGO), C.byref(OP_BGO_ESR), C.byref(ro), C.byref(TB80),
             P(a["sx"]) if a["sx"] else None, None, None, None, None, None, a["n_src"], a["n_photons"],
             1, 0, 1768.0, 100000, None, None, None, None, None, None, None, a["n_sites"], 2,
             a["n_segments"], P(a["maps"]), P(a["tmin"]), P(a["npe"]), P(a["ctr"]), None, None)
@@ -33,7 +33,7 @@ def test_events_surrogate_rejects_bad_arguments(engine):
     assert call(n_sites=4) == _lib.CL_ERR_ARG                       # null site arrays
     assert call(maps=0) == _lib.CL_ERR_ARG
     # the handle still works
-    res = engine.run_segments(BOX_BGO, OP_C2, GRID, TB80, sources=[(24.0, 24.0, 11.2)], photons_per_source=[500],
+    res = engine.run_segments(BOX_BGO, OP_BGO_ESR, GRID, TB80, sources=[(24.0, 24.0, 11.2)], photons_per_source=[500],
                               segment_of_source=[0], n_segments=1, seed=1, tau_ns=0.0)
     assert res.counters["ndet"] + res.counters["nabs_bulk"] + res.counters["nabs_wall"] + \
         res.counters["nabs_sipm"] + res.counters["ncap"] == 500
@@ -86,13 +86,13 @@ def test_sampled_site_with_a_bad_segment_is_skipped_and_reported(engine):
     light = SiteLight(p, torch.full((n, 64), 2.0, device="cuda"), torch.full((n, 64), 0.5, device="cuda"),
                       torch.zeros(n, device="cuda"), torch.zeros(n, dtype=torch.uint8, device="cuda"))
     with pytest.raises(CudaTransportError) as e:
-        sample_sites(engine, BOX_BGO, OP_C2, GRID, TB80, xyz=xyz, t0=t0, photons=ph, segment=seg,
+        sample_sites(engine, BOX_BGO, OP_BGO_ESR, GRID, TB80, xyz=xyz, t0=t0, photons=ph, segment=seg,
                      n_segments=2, seed=3, tau_ns=1768.0, light=light)
     assert e.value.code == _lib.CL_ERR_ARG and b"segment" in engine.lib.cl_last_error(engine.handle)
     # valid ids go through afterwards
     seg[2] = 0
     (maps, tmin, npe, ctr, sampled), st = sample_sites(
-        engine, BOX_BGO, OP_C2, GRID, TB80, xyz=xyz, t0=t0, photons=ph, segment=seg, n_segments=2, seed=3,
+        engine, BOX_BGO, OP_BGO_ESR, GRID, TB80, xyz=xyz, t0=t0, photons=ph, segment=seg, n_segments=2, seed=3,
         tau_ns=1768.0, light=light)
     assert int(sampled[0]) == 4000 and int(npe.sum()) == int(sampled[1]) > 0
 
@@ -115,7 +115,7 @@ def test_transport_source_with_a_bad_segment_is_reported(engine):
     npe = torch.zeros(2, dtype=torch.int32, device=dev)
     ctr = torch.zeros(9, dtype=torch.int64, device=dev)
     st = torch.cuda.Stream()
-    engine.run_segments_device(BOX_BGO, OP_C2, GRID, TB80, sx=sx.data_ptr(), sy=sy.data_ptr(), sz=sz.data_ptr(),
+    engine.run_segments_device(BOX_BGO, OP_BGO_ESR, GRID, TB80, sx=sx.data_ptr(), sy=sy.data_ptr(), sz=sz.data_ptr(),
                                st=None, src_offsets=off.data_ptr(), src_segment=seg.data_ptr(), n_src=2,
                                n_segments=2, n_photons=1000, seed=4, tau_ns=0.0, maps=maps.data_ptr(),
                                tmin=tmin.data_ptr(), npe=npe.data_ptr(), counters=ctr.data_ptr(),

@@ -5,7 +5,7 @@ high-statistics light response against the Monte Carlo of the same sites."""
 import numpy as np
 import pytest
 
-from cases import BOX_BGO, GRID, OP_C2, TB80, TAU_C2, scan_points
+from cases import BOX_BGO, GRID, OP_BGO_ESR, TB80, TAU_BGO, scan_points
 
 pytestmark = pytest.mark.gpu
 
@@ -130,7 +130,7 @@ def _light_from_scan(engine, pts, photons, per_site_rows, pde):
     from crysplight_b200 import _lib
     from crysplight_b200.fast_events import SiteLight
     from crysplight_b200.surrogate import scan_light
-    scan = scan_light(engine, BOX_BGO, OP_C2, GRID, points=pts, photons_per_point=photons, seed=77)
+    scan = scan_light(engine, BOX_BGO, OP_BGO_ESR, GRID, points=pts, photons_per_point=photons, seed=77)
     c = np.maximum(scan.counts.astype(np.float64), 1)
     m1 = scan.tsum.astype(np.float64) / _lib.MOMENT_T_SCALE / c
     m2 = scan.tsum2.astype(np.float64) / _lib.MOMENT_T2_SCALE / c
@@ -147,7 +147,7 @@ def test_all_fallback_equals_the_segment_transport(engine):
     import torch
     from crysplight_b200.fast_events import SiteLight, sample_sites
     from crysplight_b200.params import OpticalParams
-    op = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, OP_C2.sigma_alpha, 0.4)
+    op = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, OP_BGO_ESR.sigma_alpha, 0.4)
     pts, xyz, t0, ph, seg = _sites(6, 3000, 4)
     n = xyz.shape[0]
     z = lambda *s: torch.zeros(*s, dtype=torch.float32, device="cuda")
@@ -155,9 +155,9 @@ def test_all_fallback_equals_the_segment_transport(engine):
     T = lambda a: torch.from_numpy(a).cuda()
     (maps, tmin, npe, ctr, sampled), st = sample_sites(
         engine, BOX_BGO, op, GRID, TB80, xyz=T(xyz), t0=T(t0), photons=T(ph), segment=T(seg),
-        n_segments=n, seed=99, tau_ns=TAU_C2, light=light)
+        n_segments=n, seed=99, tau_ns=TAU_BGO, light=light)
     ref = engine.run_segments(BOX_BGO, op, GRID, TB80, sources=xyz, photons_per_source=ph,
-                              segment_of_source=seg, n_segments=n, seed=99, t0s=t0, tau_ns=TAU_C2)
+                              segment_of_source=seg, n_segments=n, seed=99, t0s=t0, tau_ns=TAU_BGO)
     m = maps.cpu().numpy().view(np.uint32).reshape(n, 64).T
     assert np.array_equal(m, ref.maps.reshape(64, n, order="F"))
     assert np.array_equal(tmin.cpu().numpy().reshape(n, 64).T.view(np.uint32),
@@ -174,7 +174,7 @@ def test_sampling_reproduces_the_monte_carlo(engine):
     import torch
     from crysplight_b200.fast_events import compare_maps, sample_sites
     from crysplight_b200.params import OpticalParams
-    op = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, OP_C2.sigma_alpha, 0.4)
+    op = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, OP_BGO_ESR.sigma_alpha, 0.4)
     n_pts, per = 6, 300
     pts, xyz, t0, ph, seg = _sites(n_pts, 4000, per, seed=8)
     n = xyz.shape[0]
@@ -182,14 +182,14 @@ def test_sampling_reproduces_the_monte_carlo(engine):
     T = lambda a: torch.from_numpy(a).cuda()
     (maps, tmin, npe, ctr, sampled), st = sample_sites(
         engine, BOX_BGO, op, GRID, TB80, xyz=T(xyz), t0=T(t0), photons=T(ph), segment=T(seg),
-        n_segments=n, seed=12, tau_ns=TAU_C2, light=light)
+        n_segments=n, seed=12, tau_ns=TAU_BGO, light=light)
     assert st["fallback_sites"] == 0
     s_maps = maps.cpu().numpy().view(np.uint32).reshape(n, 64).astype(np.int64)
     s_tmin = tmin.cpu().numpy().reshape(n, 64)
     assert int(sampled[0]) == int(ph.sum()) and int(sampled[1]) == int(s_maps.sum())
     assert np.array_equal(npe.cpu().numpy(), s_maps.sum(1))
     ref = engine.run_segments(BOX_BGO, op, GRID, TB80, sources=xyz, photons_per_source=ph,
-                              segment_of_source=seg, n_segments=n, seed=5, t0s=t0, tau_ns=TAU_C2)
+                              segment_of_source=seg, n_segments=n, seed=5, t0s=t0, tau_ns=TAU_BGO)
     m_maps = ref.maps.reshape(64, n, order="F").T.astype(np.int64)
     m_tmin = ref.tmin.reshape(64, n, order="F").T
     for k in range(n_pts):

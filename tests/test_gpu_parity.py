@@ -13,8 +13,8 @@ import pytest
 
 from crysplight_b200.params import (Box, OpticalParams, Readout, SipmGrid, TimeBinning,
                                     deg2rad_f32)
-from cases import (BOX_BGO, BOX_CSI, CENTRE_BGO, CENTRE_CSI, GRID, INF, OP_ALL, OP_BENCH, OP_C1,
-                   OP_C2, RO_ALL, TAU_C1, TAU_C2, TB, TB80, ideal, scan_points)
+from cases import (BOX_BGO, BOX_CSI, CENTRE_BGO, CENTRE_CSI, GRID, INF, OP_ALL, OP_BENCH, OP_CSI_TEFLON,
+                   OP_BGO_ESR, RO_ALL, TAU_CSI, TAU_BGO, TB, TB80, ideal, scan_points)
 
 pytestmark = pytest.mark.gpu
 NT = os.cpu_count() or 1
@@ -124,10 +124,10 @@ def test_math_special_values(engine, oracle):
 # ---- transport: per-photon records ------------------------------------------------------
 CASES = {
     # name: (box, op, readout, tb, kwargs)
-    "config1_csitl_teflon": (BOX_CSI, OP_C1, Readout(GRID), TB80,
-                             dict(n_photons=200_000, seed=1234, pos=CENTRE_CSI, tau_ns=TAU_C1)),
-    "config2_bgo_esr_centre": (BOX_BGO, OP_C2, Readout(GRID), TB80,
-                               dict(n_photons=100_000, seed=1234, pos=CENTRE_BGO, tau_ns=TAU_C2)),
+    "point_csitl_teflon": (BOX_CSI, OP_CSI_TEFLON, Readout(GRID), TB80,
+                             dict(n_photons=200_000, seed=1234, pos=CENTRE_CSI, tau_ns=TAU_CSI)),
+    "point_bgo_esr_centre": (BOX_BGO, OP_BGO_ESR, Readout(GRID), TB80,
+                               dict(n_photons=100_000, seed=1234, pos=CENTRE_BGO, tau_ns=TAU_BGO)),
     "all_processes_disc_surround": (BOX_CSI, OP_ALL, RO_ALL, TB,
                                     dict(n_photons=100_000, seed=8, pos=CENTRE_CSI, tau_ns=800.0)),
     "all_processes_two_sided": (BOX_CSI, OP_ALL, Readout(GRID, two_sided=True), TB,
@@ -150,10 +150,10 @@ CASES = {
                                                    (3.0, 40.0, 1.0)],
                                         t0s=[0.0, 55.5, 7000.0], pid_offset=123_456_789,
                                         tau_ns=800.0)),
-    "source_outside_crystal": (BOX_CSI, OP_C1, Readout(GRID), TB80,
+    "source_outside_crystal": (BOX_CSI, OP_CSI_TEFLON, Readout(GRID), TB80,
                                dict(n_photons=20_000, seed=5, positions=[(-3.0, 24.0, 10.0),
                                                                           (24.0, 60.0, 40.0)],
-                                    tau_ns=TAU_C1)),
+                                    tau_ns=TAU_CSI)),
     "cap_and_overflow": (BOX_CSI, ideal(1.95), Readout(GRID), TimeBinning(1.0, 3),
                          dict(n_photons=20_000, seed=2, pos=CENTRE_CSI, tau_ns=0.0,
                               max_bounces=50)),
@@ -177,7 +177,7 @@ def test_transport_matches_oracle(engine, oracle, name):
 def test_accumulator_without_records_matches(engine, oracle):
     """The tile path (no records) produces the same Accumulator as the oracle's
     threaded run_photons! (src/transport.jl:245-273)."""
-    box, op, ro, tb, kw = CASES["config1_csitl_teflon"]
+    box, op, ro, tb, kw = CASES["point_csitl_teflon"]
     dacc = engine.run_photons(box, op, ro, tb, n_photons=kw["n_photons"], seed=kw["seed"],
                               pos=kw["pos"], tau_ns=kw["tau_ns"])
     oacc = oracle.run_photons(box, op, ro, tb, n_photons=kw["n_photons"], seed=kw["seed"],
@@ -200,19 +200,19 @@ def test_global_tile_path_for_long_histograms(engine, oracle):
     """A histogram too large for shared memory takes the global-atomics path."""
     tb = TimeBinning(0.5, 60_000)      # 64 x 60001 bins > shared memory
     kw = dict(n_photons=30_000, seed=77, pos=CENTRE_CSI, tau_ns=1000.0)
-    d = engine.run_photons_ka(BOX_CSI, OP_C1, Readout(GRID), tb, **kw)
-    o = oracle.run_photons_ka(BOX_CSI, OP_C1, Readout(GRID), tb, nthreads=NT, **kw)
+    d = engine.run_photons_ka(BOX_CSI, OP_CSI_TEFLON, Readout(GRID), tb, **kw)
+    o = oracle.run_photons_ka(BOX_CSI, OP_CSI_TEFLON, Readout(GRID), tb, nthreads=NT, **kw)
     _assert_acc_equal(d, o)
 
 
 def test_empty_and_single_photon(engine, oracle):
-    acc = engine.run_photons_ka(BOX_CSI, OP_C1, GRID, TB, n_photons=0, seed=1, pos=CENTRE_CSI,
+    acc = engine.run_photons_ka(BOX_CSI, OP_CSI_TEFLON, GRID, TB, n_photons=0, seed=1, pos=CENTRE_CSI,
                                 tau_ns=1000.0)
     assert acc.counts.sum() == 0 and np.all(np.isinf(acc.first_ns)) and acc.total_terminated() == 0
     for seed in (1, 2, 3):
-        d, dr = engine.run_photons_ka(BOX_CSI, OP_C1, GRID, TB, n_photons=1, seed=seed,
+        d, dr = engine.run_photons_ka(BOX_CSI, OP_CSI_TEFLON, GRID, TB, n_photons=1, seed=seed,
                                       pos=CENTRE_CSI, tau_ns=1000.0, return_records=True)
-        o, orr = oracle.run_photons_ka(BOX_CSI, OP_C1, GRID, TB, n_photons=1, seed=seed,
+        o, orr = oracle.run_photons_ka(BOX_CSI, OP_CSI_TEFLON, GRID, TB, n_photons=1, seed=seed,
                                        pos=CENTRE_CSI, tau_ns=1000.0, return_records=True)
         _assert_acc_equal(d, o)
         assert dr.status[0] == orr.status[0] and dr.t[0] == orr.t[0]
@@ -221,16 +221,16 @@ def test_empty_and_single_photon(engine, oracle):
 def test_bad_arguments_are_rejected(engine):
     from crysplight_b200._lib import CudaTransportError
     with pytest.raises(CudaTransportError):
-        engine.run_photons_ka(Box((48, 48, -1)), OP_C1, GRID, TB, n_photons=10, seed=1,
+        engine.run_photons_ka(Box((48, 48, -1)), OP_CSI_TEFLON, GRID, TB, n_photons=10, seed=1,
                               pos=CENTRE_CSI, tau_ns=0.0)
     with pytest.raises(CudaTransportError):
-        engine.run_photons_ka(BOX_CSI, OP_C1, SipmGrid(6, 300, 300), TB, n_photons=10, seed=1,
+        engine.run_photons_ka(BOX_CSI, OP_CSI_TEFLON, SipmGrid(6, 300, 300), TB, n_photons=10, seed=1,
                               pos=CENTRE_CSI, tau_ns=0.0)
     with pytest.raises(CudaTransportError):
-        engine.run_photons_ka(BOX_CSI, OP_C1, GRID, TimeBinning(0.0, 10), n_photons=10, seed=1,
+        engine.run_photons_ka(BOX_CSI, OP_CSI_TEFLON, GRID, TimeBinning(0.0, 10), n_photons=10, seed=1,
                               pos=CENTRE_CSI, tau_ns=0.0)
     # the handle is still usable afterwards
-    acc = engine.run_photons_ka(BOX_CSI, OP_C1, GRID, TB, n_photons=1000, seed=1,
+    acc = engine.run_photons_ka(BOX_CSI, OP_CSI_TEFLON, GRID, TB, n_photons=1000, seed=1,
                                 pos=CENTRE_CSI, tau_ns=0.0)
     assert acc.total_terminated() == 1000
 
@@ -251,8 +251,8 @@ def test_segments_match_oracle(engine, oracle):
     src, counts, seg, t0 = _segment_case(rng)
     kw = dict(sources=src, photons_per_source=counts, segment_of_source=seg, n_segments=40,
               seed=11, t0s=t0, pid_offset=1000, tau_ns=1000.0)
-    dres, drec = engine.run_segments(BOX_CSI, OP_C1, GRID, TB80, return_records=True, **kw)
-    ores, orec = oracle.run_segments(BOX_CSI, OP_C1, GRID, TB80, return_records=True,
+    dres, drec = engine.run_segments(BOX_CSI, OP_CSI_TEFLON, GRID, TB80, return_records=True, **kw)
+    ores, orec = oracle.run_segments(BOX_CSI, OP_CSI_TEFLON, GRID, TB80, return_records=True,
                                      nthreads=NT, **kw)
     nonexact = _assert_records_equal(drec, orec)
     assert dres.counters["ndet"] == int(dres.npe.sum())
@@ -270,35 +270,35 @@ def test_segments_equal_point_runs(engine):
     per point with pid_offset = photons before it gives."""
     pts = scan_points(5, BOX_BGO, seed=7)
     per = 20_000
-    res = engine.run_segments(BOX_BGO, OP_C2, GRID, TB80, sources=pts,
+    res = engine.run_segments(BOX_BGO, OP_BGO_ESR, GRID, TB80, sources=pts,
                               photons_per_source=[per] * 5, segment_of_source=range(5),
-                              n_segments=5, seed=1234, tau_ns=TAU_C2)
+                              n_segments=5, seed=1234, tau_ns=TAU_BGO)
     for p in range(5):
-        acc = engine.run_photons_ka(BOX_BGO, OP_C2, GRID, TB80, n_photons=per, seed=1234,
-                                    pos=tuple(pts[p]), pid_offset=p * per, tau_ns=TAU_C2)
+        acc = engine.run_photons_ka(BOX_BGO, OP_BGO_ESR, GRID, TB80, n_photons=per, seed=1234,
+                                    pos=tuple(pts[p]), pid_offset=p * per, tau_ns=TAU_BGO)
         assert np.array_equal(acc.counts.sum(axis=2), res.maps[:, :, p])
         assert np.array_equal(acc.first_ns.view(np.uint32), res.tmin[:, :, p].view(np.uint32))
         assert acc.ndet == res.npe[p]
 
 
 # ---- full workload sizes (10^6 photons; 51.2M photons): exact where the oracle is fast, properties otherwise
-def test_config1_full_size_exact(engine, oracle):
-    """Config 1 at its full 1,000,000 photons: identical to the oracle."""
-    kw = dict(n_photons=1_000_000, seed=1234, pos=CENTRE_CSI, tau_ns=TAU_C1)
-    d = engine.run_photons(BOX_CSI, OP_C1, GRID, TB80, **kw)
-    o = oracle.run_photons(BOX_CSI, OP_C1, GRID, TB80, nthreads=NT, **kw)
+def test_point_source_csitl_full_size_exact(engine, oracle):
+    """The CsI(Tl)+Teflon point source at its full 1,000,000 photons: identical to the oracle."""
+    kw = dict(n_photons=1_000_000, seed=1234, pos=CENTRE_CSI, tau_ns=TAU_CSI)
+    d = engine.run_photons(BOX_CSI, OP_CSI_TEFLON, GRID, TB80, **kw)
+    o = oracle.run_photons(BOX_CSI, OP_CSI_TEFLON, GRID, TB80, nthreads=NT, **kw)
     _assert_acc_equal(d, o)
     assert abs(d.ndet / 1e6 - 0.888) < 0.002
 
 
-def test_config2_full_size_properties(engine, oracle):
-    """Config 2 at full size: 256 points x 200,000 photons (51.2M).  Size-
+def test_bgo_esr_scan_full_size_properties(engine, oracle):
+    """The BGO+ESR scan at full size: 256 points x 200,000 photons (51.2M).  Size-
     independent properties on the whole run; exact equality on 4 points."""
     pts = scan_points(256, BOX_BGO, seed=7)
     per = 200_000
-    res = engine.run_segments(BOX_BGO, OP_C2, GRID, TB80, sources=pts,
+    res = engine.run_segments(BOX_BGO, OP_BGO_ESR, GRID, TB80, sources=pts,
                               photons_per_source=[per] * 256, segment_of_source=range(256),
-                              n_segments=256, seed=1234, tau_ns=TAU_C2)
+                              n_segments=256, seed=1234, tau_ns=TAU_BGO)
     c = res.counters
     assert sum(c[k] for k in ("ndet", "nabs_bulk", "nabs_wall", "nabs_sipm", "ncap",
                               "nabs_sur")) == 256 * per
@@ -308,9 +308,9 @@ def test_config2_full_size_properties(engine, oracle):
     frac = res.npe / per
     assert 0.3 < frac.min() and frac.max() < 0.95
     for p in (0, 17, 128, 255):
-        sub = oracle.run_segments(BOX_BGO, OP_C2, GRID, TB80, sources=pts[p:p + 1],
+        sub = oracle.run_segments(BOX_BGO, OP_BGO_ESR, GRID, TB80, sources=pts[p:p + 1],
                                   photons_per_source=[per], segment_of_source=[0], n_segments=1,
-                                  seed=1234, pid_offset=p * per, tau_ns=TAU_C2, nthreads=NT)
+                                  seed=1234, pid_offset=p * per, tau_ns=TAU_BGO, nthreads=NT)
         assert np.array_equal(sub["maps"][:, :, 0], res.maps[:, :, p])
         assert np.array_equal(sub["tmin"][:, :, 0].view(np.uint32),
                               res.tmin[:, :, p].view(np.uint32))

@@ -8,7 +8,7 @@ the two paths must be identical."""
 import numpy as np
 import pytest
 
-from cases import BOX_BGO, BOX_CSI, GRID, OP_C1, OP_C2, TB80, scan_points
+from cases import BOX_BGO, BOX_CSI, GRID, OP_CSI_TEFLON, OP_BGO_ESR, TB80, scan_points
 
 pytestmark = pytest.mark.gpu
 
@@ -34,7 +34,7 @@ def _fixed_sums(recs, per, n_points, cells):
 @pytest.mark.parametrize("case", ["bgo_esr", "csitl_teflon"])
 def test_scan_moments_exact(engine, case):
     from crysplight_b200.surrogate import scan_light
-    box, op = (BOX_BGO, OP_C2) if case == "bgo_esr" else (BOX_CSI, OP_C1)
+    box, op = (BOX_BGO, OP_BGO_ESR) if case == "bgo_esr" else (BOX_CSI, OP_CSI_TEFLON)
     pts = scan_points(6, box, seed=5)
     per = 4000
     scan = scan_light(engine, box, op, GRID, points=pts, photons_per_point=per, seed=21,
@@ -57,7 +57,7 @@ def test_scan_moments_exact(engine, case):
 def test_targets_from_scan(engine):
     from crysplight_b200.surrogate import light_targets, scan_light
     pts = scan_points(4, BOX_BGO, seed=9)
-    scan = scan_light(engine, BOX_BGO, OP_C2, GRID, points=pts, photons_per_point=50_000, seed=3)
+    scan = scan_light(engine, BOX_BGO, OP_BGO_ESR, GRID, points=pts, photons_per_point=50_000, seed=3)
     y = light_targets(scan)
     assert y.shape == (4, 192) and np.isfinite(y).all()
     p = np.exp(y[:, :64])

@@ -10,8 +10,8 @@ from crysplight_b200.params import (Accumulator, Box, OpticalParams, Readout, Si
                                     TimeBinning, FACE_BACK, FACE_FRONT, FACE_XM, FACE_XP,
                                     FACE_YM, FACE_YP, STATUS_ABS_SUR, STATUS_DETECTED,
                                     deg2rad_f32, surface_has_gap)
-from cases import (BOX_BGO, BOX_CSI, CENTRE_CSI, GRID, INF, OP_ALL, OP_C1, RO_ALL, TB, TB80,
-                   TAU_C1, ideal)
+from cases import (BOX_BGO, BOX_CSI, CENTRE_CSI, GRID, INF, OP_ALL, OP_CSI_TEFLON, RO_ALL, TB, TB80,
+                   TAU_CSI, ideal)
 
 
 def test_configuration_validation():            # test/runtests.jl:11-15
@@ -250,12 +250,12 @@ def test_detection_record(oracle):                  # test/runtests.jl:341-357
     assert acc.acc.counts[1, 6, -1] == 1
 
 
-def test_published_physics_config1(oracle):
+def test_published_physics_csitl_teflon(oracle):
     """latex/csitl_calib.tex:300-308: CsI(Tl)+Teflon centre, PDE 1: 88.8%
     detected, 10.0% bulk, 1.2% wall (quoted to 0.1%)."""
     n = 400_000
-    acc = oracle.run_photons(BOX_CSI, OP_C1, GRID, TB80, n_photons=n, seed=1234,
-                             pos=CENTRE_CSI, tau_ns=TAU_C1)
+    acc = oracle.run_photons(BOX_CSI, OP_CSI_TEFLON, GRID, TB80, n_photons=n, seed=1234,
+                             pos=CENTRE_CSI, tau_ns=TAU_CSI)
     assert abs(acc.ndet / n - 0.888) < 0.0015
     assert abs(acc.nabs_bulk / n - 0.100) < 0.0015
     assert abs(acc.nabs_wall / n - 0.012) < 0.0015

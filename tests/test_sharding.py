@@ -9,7 +9,7 @@ import socket
 import numpy as np
 import pytest
 
-from cases import BOX_CSI, GRID, OP_ALL, OP_C1, TB, TB80, scan_points
+from cases import BOX_CSI, GRID, OP_ALL, OP_CSI_TEFLON, TB, TB80, scan_points
 
 
 def _free_port():
@@ -45,7 +45,7 @@ def _worker(rank, world, port, outdir):
             npos=len(POINT["positions"]), **POINT)
         pts, cnt, seg, n_seg, t0 = _events()
         maps, tmin, npe, ctr = sharding.run_segments_sharded(
-            lambda **kw: oracle.run_segments(BOX_CSI, OP_C1, GRID, TB80, nthreads=2, seed=5, tau_ns=1000.0,
+            lambda **kw: oracle.run_segments(BOX_CSI, OP_CSI_TEFLON, GRID, TB80, nthreads=2, seed=5, tau_ns=1000.0,
                                              **kw),
             sources=pts, photons_per_source=cnt, segment_of_source=seg, n_segments=n_seg, t0s=t0)
         np.savez(os.path.join(outdir, f"rank{rank}.npz"), counts=acc.counts, first=acc.first_ns,
@@ -85,7 +85,7 @@ def test_sharded_point_source_equals_single_run(sharded, oracle):
 
 def test_sharded_events_equal_single_run(sharded, oracle):
     pts, cnt, seg, n_seg, t0 = _events()
-    ref = oracle.run_segments(BOX_CSI, OP_C1, GRID, TB80, sources=pts, photons_per_source=cnt,
+    ref = oracle.run_segments(BOX_CSI, OP_CSI_TEFLON, GRID, TB80, sources=pts, photons_per_source=cnt,
                               segment_of_source=seg, n_segments=n_seg, t0s=t0, seed=5, tau_ns=1000.0,
                               nthreads=4)
     for r in sharded:

@@ -18,7 +18,7 @@ import pytest
 
 from crysplight_b200 import _lib
 from crysplight_b200.params import Accumulator, Counters, Readout, TimeBinning
-from cases import BOX_CSI, CENTRE_CSI, GRID, OP_ALL, OP_C1, RO_ALL, TAU_C1, TB, TB80
+from cases import BOX_CSI, CENTRE_CSI, GRID, OP_ALL, OP_CSI_TEFLON, RO_ALL, TAU_CSI, TB, TB80
 
 pytestmark = pytest.mark.gpu
 
@@ -53,8 +53,8 @@ def _same(a, b):
 
 def test_noalloc_matches_regular_entry_point_twice(engine):
     calls = [
-        (BOX_CSI, OP_C1, Readout(GRID), TB80,
-         dict(n_photons=200_000, seed=1234, positions=[CENTRE_CSI], tau_ns=TAU_C1)),
+        (BOX_CSI, OP_CSI_TEFLON, Readout(GRID), TB80,
+         dict(n_photons=200_000, seed=1234, positions=[CENTRE_CSI], tau_ns=TAU_CSI)),
         (BOX_CSI, OP_ALL, RO_ALL, TB,
          dict(n_photons=100_000, seed=8, positions=[(24.0, 24.0, 5.0), (24.0, 24.0, 30.0)],
               t0s=[0.0, 40.0], pid_offset=777, tau_ns=800.0)),
@@ -71,14 +71,14 @@ def test_noalloc_matches_regular_entry_point_twice(engine):
 
 def test_noalloc_refuses_requests_larger_than_its_array(engine):
     big = TimeBinning(1.0, SCRATCH_BYTES // (4 * 64))   # 64 cells x (nbins+1) words > 1 MiB
-    rc, msg, _ = _noalloc(BOX_CSI, OP_C1, GRID, big, n_photons=10, seed=1,
+    rc, msg, _ = _noalloc(BOX_CSI, OP_CSI_TEFLON, GRID, big, n_photons=10, seed=1,
                           positions=[CENTRE_CSI], tau_ns=0.0)
     assert rc == _lib.CL_ERR_ARG
     assert "static device array" in msg
     # the array is still usable afterwards, and a later call leaves nothing behind
-    rc, msg, a = _noalloc(BOX_CSI, OP_C1, GRID, TB, n_photons=5_000, seed=3,
+    rc, msg, a = _noalloc(BOX_CSI, OP_CSI_TEFLON, GRID, TB, n_photons=5_000, seed=3,
                           positions=[CENTRE_CSI], tau_ns=0.0)
     assert rc == _lib.CL_OK, msg
-    ref = engine.run_photons_ka(BOX_CSI, OP_C1, GRID, TB, n_photons=5_000, seed=3,
+    ref = engine.run_photons_ka(BOX_CSI, OP_CSI_TEFLON, GRID, TB, n_photons=5_000, seed=3,
                                 pos=CENTRE_CSI, tau_ns=0.0)
     _same(a, ref)
