@@ -70,12 +70,13 @@ inline void put(Bytes& o, uint64_t v, int n)
 inline void put(Bytes& o, const Bytes& b) { o.insert(o.end(), b.begin(), b.end()); }
 
 // Element types of datasets and attributes.
-enum class Type { U8, I32, U32, I64, U64, F32, F64, Str };
+enum class Type { I8, U8, I16, U16, I32, U32, I64, U64, F32, F64, Str };
 
 inline int type_size(Type t)
 {
     switch (t) {
-    case Type::U8: return 1;
+    case Type::I8: case Type::U8: return 1;
+    case Type::I16: case Type::U16: return 2;
     case Type::I32: case Type::U32: case Type::F32: return 4;
     case Type::I64: case Type::U64: case Type::F64: return 8;
     default: return 0;
@@ -108,7 +109,7 @@ inline Bytes datatype(Type t, uint32_t strlen = 0)
         put(o, d ? 1023 : 127, 4);          // exponent bias
         return o;
     }
-    const bool is_signed = t == Type::I32 || t == Type::I64;
+    const bool is_signed = t == Type::I8 || t == Type::I16 || t == Type::I32 || t == Type::I64;
     o.push_back((1 << 4) | 0);
     o.push_back(is_signed ? 0x08 : 0); o.push_back(0); o.push_back(0);
     put(o, (uint64_t)size, 4);

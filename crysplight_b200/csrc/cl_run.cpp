@@ -1,17 +1,28 @@
-// cl_run.cpp — `crysplight_run`: point-source runs from CryspLight's run files
-// through the C-ABI alone (no Python, no Julia), the counterpart of
-// scripts/run_point_source.jl → run_from_config (src/config.jl:72-79).
+// cl_run.cpp — `crysplight_run`: CryspLight's run files through the C-ABI
+// alone (no Python, no Julia), the counterpart of both of the reference's
+// run scripts:
 //
 //   crysplight_run [--device N] [--data DIR] [--output-root DIR]
-//                  [--n-photons N] [--print-setup] [--no-write] run.toml ...
+//                  [--n-photons N] [--n-events N] [--print-setup] [--no-write]
+//                  run.toml ...
 //
-// For each run file: load_setup (src/config.jl:27-69) with the materials of
-// data/<name>.toml (the run file's ../data, else the package's data
+// A point-source run file (scripts/run_point_source.jl → run_from_config,
+// src/config.jl:72-79): load_setup (src/config.jl:27-69) with the materials
+// of data/<name>.toml (the run file's ../data, else the package's data
 // directory), one cl_run_photons call, the reference's summary lines
 // (src/output.jl:36-52), and output/<tag>/light.h5 plus a copy of the run
-// file (src/output.jl:10-32).  --print-setup prints the parsed setup as JSON
-// and runs nothing (no GPU needed).
+// file (src/output.jl:10-32).
+//
+// A gamma campaign (a run file with a [campaign] table;
+// scripts/shoot_gammas.jl:19-90): the gamma material from [gamma] density and
+// its XCOM table, the gamma stage of every event on the host
+// (cl_gamma_events), every deposit's photons in one cl_run_segments call, the
+// reference's summary, and output/<tag>/events.h5 plus a copy of the run file.
+//
+// --print-setup prints the parsed setup as JSON and runs nothing (no GPU
+// needed).
 #include <cerrno>
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -353,11 +364,252 @@ int run_one(cl_handle* h, const Setup& s, bool write)
     return 0;
 }
 
+// ---- gamma campaigns, scripts/shoot_gammas.jl:19-90 ----
+struct GammaSetup {
+    std::string tag, cfg_path, outdir, crystal_name, xcom_path;
+    cl_box box{};
+    cl_optical_params op{};
+    cl_readout ro{};
+    cl_time_binning tb{};
+    double yield_per_mev = 0.0, density = 0.0;
+    float tau_ns = 0.0f;
+    int64_t n_events = 0;
+    uint64_t seed = 0;
+};
+
+GammaSetup load_gamma_setup(const std::string& cfg_arg, const std::string& data_override,
+                            const std::string& out_root)
+{
+    GammaSetup g;
+    g.cfg_path = absolute(cfg_arg);
+    const Document cfg = cltoml::parse_file(g.cfg_path);
+    const std::string root = dirname_of(dirname_of(g.cfg_path));
+    std::string data_dir = data_override;
+    if (data_dir.empty()) data_dir = is_dir(join(root, "data")) ? join(root, "data") : package_data_dir();
+    const Table& camp = table(cfg, "campaign", g.cfg_path);
+    g.tag = str(need(camp, "tag", "[campaign]"), "campaign.tag");
+    g.n_events = integer(need(camp, "n_events", "[campaign]"), "campaign.n_events");
+    g.seed = (uint64_t)integer(need(camp, "seed", "[campaign]"), "campaign.seed");
+    const Table& crystal_cfg = table(cfg, "crystal", g.cfg_path);
+    g.crystal_name = str(need(crystal_cfg, "material", "[crystal]"), "crystal.material");
+    const std::string wrap_name = str(need(table(cfg, "wrap", g.cfg_path), "material", "[wrap]"), "wrap.material");
+    const Table& sipm_cfg = table(cfg, "sipm", g.cfg_path);
+    const std::string sipm_name = str(need(sipm_cfg, "material", "[sipm]"), "sipm.material");
+    const Document crystal = load_material(g.crystal_name, data_dir);
+    const Document wrap = load_material(wrap_name, data_dir);
+    const Document sipm = load_material(sipm_name, data_dir);
+    const Table& C = crystal.at("");
+    const Table& W = wrap.at("");
+    const Table& S = sipm.at("");
+    const std::vector<double> sz = vec3(need(crystal_cfg, "size_mm", "[crystal]"), "crystal.size_mm");
+    for (int i = 0; i < 3; ++i) g.box.L[i] = (float)sz[i];
+    const Table& surf = table(cfg, "surface", g.cfg_path);
+    const Value* fin = find(surf, "finish");
+    const std::string finish = fin ? str(*fin, "surface.finish") : "backpainted";
+    if (finish != "backpainted" && finish != "frontpainted") throw std::runtime_error("unknown finish: " + finish);
+    g.op.n_crystal = (float)num(need(C, "n", g.crystal_name), "n");
+    g.op.n_coupling = (float)num(need(sipm_cfg, "coupling_n", "[sipm]"), "coupling_n");
+    g.op.abs_len_mm = (float)num(need(C, "abs_length_mm", g.crystal_name), "abs_length_mm");
+    const Value* ray = find(C, "rayleigh_mm");
+    g.op.rayleigh_mm = ray ? (float)num(*ray, "rayleigh_mm") : INFINITY;
+    g.op.wrap_R = (float)num(need(W, "reflectivity", wrap_name), "reflectivity");
+    g.op.wrap_specular = str(need(W, "model", wrap_name), "model") == "specular" ? 1 : 0;
+    g.op.air_gap = finish == "backpainted" ? 1 : 0;
+    g.op.sigma_alpha = (float)(num(need(surf, "sigma_alpha_deg", "[surface]"), "surface.sigma_alpha_deg") *
+                               (M_PI / 180.0));
+    const Value* pde_o = find(sipm_cfg, "pde_override");
+    g.op.pde = (float)num(pde_o ? *pde_o : need(S, "pde", sipm_name), "pde");
+    g.ro.grid.pitch_mm = (float)num(need(S, "pitch_mm", sipm_name), "pitch_mm");
+    g.ro.grid.nx = (int32_t)integer(need(S, "nx", sipm_name), "nx");
+    g.ro.grid.ny = (int32_t)integer(need(S, "ny", sipm_name), "ny");
+    const Table& bin = table(cfg, "binning", g.cfg_path);
+    g.tb.bin_ns = (float)num(need(bin, "bin_ns", "[binning]"), "bin_ns");
+    g.tb.nbins = (int32_t)std::nearbyint(num(need(bin, "window_ns", "[binning]"), "window_ns") / (double)g.tb.bin_ns);
+    g.yield_per_mev = num(need(C, "yield_per_mev", g.crystal_name), "yield_per_mev");
+    g.tau_ns = (float)num(need(C, "tau_ns", g.crystal_name), "tau_ns");
+    const Table& gam = table(cfg, "gamma", g.cfg_path);
+    g.density = num(need(gam, "density", "[gamma]"), "gamma.density");
+    g.xcom_path = join(data_dir, str(need(gam, "xcom", "[gamma]"), "gamma.xcom"));
+    g.outdir = join(join(out_root.empty() ? root : out_root, "output"), g.tag);
+    return g;
+}
+
+void print_gamma_setup(const GammaSetup& g)
+{
+    std::printf("{\"tag\": %s, \"cfg_path\": %s, \"outdir\": %s, \"box\": [%s, %s, %s], ",
+                json_str(g.tag).c_str(), json_str(g.cfg_path).c_str(), json_str(g.outdir).c_str(),
+                jf(g.box.L[0]).c_str(), jf(g.box.L[1]).c_str(), jf(g.box.L[2]).c_str());
+    std::printf("\"op\": {\"n_crystal\": %s, \"n_coupling\": %s, \"abs_len_mm\": %s, \"rayleigh_mm\": %s, "
+                "\"wrap_R\": %s, \"wrap_specular\": %d, \"air_gap\": %d, \"sigma_alpha\": %s, \"pde\": %s}, ",
+                jf(g.op.n_crystal).c_str(), jf(g.op.n_coupling).c_str(), jf(g.op.abs_len_mm).c_str(),
+                jf(g.op.rayleigh_mm).c_str(), jf(g.op.wrap_R).c_str(), g.op.wrap_specular, g.op.air_gap,
+                jf(g.op.sigma_alpha).c_str(), jf(g.op.pde).c_str());
+    std::printf("\"grid\": [%s, %d, %d], \"tb\": [%s, %d], \"yield_per_mev\": %s, \"tau_ns\": %s, "
+                "\"n_events\": %lld, \"seed\": %llu, \"crystal\": %s, \"density\": %s, \"xcom\": %s}\n",
+                jf(g.ro.grid.pitch_mm).c_str(), g.ro.grid.nx, g.ro.grid.ny, jf(g.tb.bin_ns).c_str(), g.tb.nbins,
+                jf(g.yield_per_mev).c_str(), jf(g.tau_ns).c_str(), (long long)g.n_events,
+                (unsigned long long)g.seed, json_str(g.crystal_name).c_str(), jf(g.density).c_str(),
+                json_str(g.xcom_path).c_str());
+}
+
+// NIST XCOM table (src/gamma/nist_data.jl:19-35): rows of 8 numbers (E,
+// coherent, incoherent, photoelectric, pair nuclear, pair electron, totals);
+// other lines are skipped.  Returns the columns E, incoherent, photoelectric,
+// pair nuclear, pair electron.
+std::vector<std::vector<double>> load_xcom(const std::string& path)
+{
+    std::ifstream f(path);
+    if (!f) throw std::runtime_error("cannot read XCOM table " + path);
+    std::vector<std::vector<double>> cols(5);
+    std::string line;
+    while (std::getline(f, line)) {
+        size_t a = line.find_first_not_of(" \t\r\n\f\v");
+        if (a == std::string::npos || line[a] < '0' || line[a] > '9') continue;
+        std::vector<std::string> fields;
+        size_t p = a;
+        while (p < line.size()) {
+            const size_t q = line.find_first_of(" \t\r\n\f\v", p);
+            fields.push_back(line.substr(p, q == std::string::npos ? std::string::npos : q - p));
+            if (q == std::string::npos) break;
+            p = line.find_first_not_of(" \t\r\n\f\v", q);
+            if (p == std::string::npos) break;
+        }
+        if (fields.size() < 8) continue;
+        double v[8];
+        for (int i = 0; i < 8; ++i) {
+            char* end = nullptr;
+            v[i] = std::strtod(fields[i].c_str(), &end);
+            if (end == fields[i].c_str() || *end != 0)
+                throw std::runtime_error(path + ": bad number '" + fields[i] + "'");
+        }
+        cols[0].push_back(v[0]); cols[1].push_back(v[2]); cols[2].push_back(v[3]);
+        cols[3].push_back(v[4]); cols[4].push_back(v[5]);
+    }
+    if (cols[0].empty()) throw std::runtime_error("no XCOM data rows in " + path);
+    return cols;
+}
+
+const char* INT_TYPE_KEY = "-1 = no interaction, 0 = direct photoelectric, X>=1 = X Compton scatters";
+
+int run_gamma(cl_handle* h, const GammaSetup& g, bool write)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    const auto xc = load_xcom(g.xcom_path);
+    cl_gamma_material* m = nullptr;
+    if (cl_gamma_material_create(&m, xc[0].data(), xc[1].data(), xc[2].data(), xc[3].data(), xc[4].data(),
+                                 (int32_t)xc[0].size(), g.density) != CL_OK) {
+        std::fprintf(stderr, "%s: %s\n", g.cfg_path.c_str(), cl_gamma_last_error());
+        return 1;
+    }
+    const int64_t n = g.n_events;
+    std::vector<float> edep(n), xyz1(3 * n), e1(n), xyz2(3 * n), e2(n), er(n);
+    std::vector<int8_t> int_type(n);
+    std::vector<int16_t> n_int(n);
+    int64_t cap = std::max<int64_t>(16, 8 * n), nd = 0;
+    std::vector<float> dep_xyz, dep_t;
+    std::vector<int32_t> dep_ev;
+    std::vector<int64_t> dep_ph;
+    for (;;) {
+        dep_xyz.assign(3 * cap, 0.0f); dep_t.assign(cap, 0.0f); dep_ev.assign(cap, 0); dep_ph.assign(cap, 0);
+        const int rc = cl_gamma_events(m, &g.box, 0, n, g.seed, 0.511, g.yield_per_mev, 0, edep.data(),
+                                       xyz1.data(), e1.data(), xyz2.data(), e2.data(), er.data(),
+                                       int_type.data(), n_int.data(), cap, dep_xyz.data(), dep_t.data(),
+                                       dep_ev.data(), dep_ph.data(), &nd);
+        if (rc == CL_OK) break;
+        if (nd > cap) { cap = nd; continue; }
+        std::fprintf(stderr, "%s: %s\n", g.cfg_path.c_str(), cl_gamma_last_error());
+        cl_gamma_material_destroy(m);
+        return 1;
+    }
+    cl_gamma_material_destroy(m);
+    const int nx = g.ro.grid.nx, ny = g.ro.grid.ny, cells = nx * ny;
+    std::vector<uint32_t> maps((size_t)cells * n, 0u);
+    std::vector<float> tmin((size_t)cells * n, INFINITY);
+    std::vector<int32_t> npe(n, 0);
+    std::vector<int64_t> off(nd + 1, 0);
+    for (int64_t i = 0; i < nd; ++i) off[i + 1] = off[i] + dep_ph[i];
+    if (nd > 0 && off[nd] > 0) {
+        std::vector<float> sx(nd), sy(nd), sz(nd);
+        for (int64_t i = 0; i < nd; ++i) { sx[i] = dep_xyz[3 * i]; sy[i] = dep_xyz[3 * i + 1]; sz[i] = dep_xyz[3 * i + 2]; }
+        cl_counters c{};
+        const int rc = cl_run_segments(h, &g.box, &g.op, &g.ro, &g.tb, sx.data(), sy.data(), sz.data(), dep_t.data(),
+                                       off.data(), dep_ev.data(), nd, n, g.seed, 0, g.tau_ns, 100000, maps.data(),
+                                       tmin.data(), npe.data(), &c, nullptr);
+        if (rc != CL_OK) {
+            std::fprintf(stderr, "%s: cl_run_segments failed (%d): %s\n", g.cfg_path.c_str(), rc, cl_last_error(h));
+            return 1;
+        }
+    }
+    std::vector<uint16_t> maps16(maps.size());
+    for (size_t i = 0; i < maps.size(); ++i) maps16[i] = (uint16_t)(maps[i] & 0xFFFFu);   // UInt16 maps wrap
+    const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (write) {
+        using namespace clh5;
+        auto raw = [](const void* p, size_t bytes) {
+            Bytes b(bytes);
+            if (bytes) std::memcpy(b.data(), p, bytes);
+            return b;
+        };
+        const uint64_t un = (uint64_t)n, ux = (uint64_t)nx, uy = (uint64_t)ny;
+        Writer w;
+        w.add_dataset({"edep_kev", Type::F32, {un}, raw(edep.data(), 4 * n)});
+        w.add_dataset({"npe", Type::I32, {un}, raw(npe.data(), 4 * n)});
+        w.add_dataset({"maps", Type::U16, {ux, uy, un}, raw(maps16.data(), 2 * maps16.size())});
+        w.add_dataset({"tmin_ns", Type::F32, {ux, uy, un}, raw(tmin.data(), 4 * tmin.size())});
+        w.add_dataset({"xyz1_mm", Type::F32, {3, un}, raw(xyz1.data(), 12 * n)});
+        w.add_dataset({"e1_kev", Type::F32, {un}, raw(e1.data(), 4 * n)});
+        w.add_dataset({"xyz2_mm", Type::F32, {3, un}, raw(xyz2.data(), 12 * n)});
+        w.add_dataset({"e2_kev", Type::F32, {un}, raw(e2.data(), 4 * n)});
+        w.add_dataset({"er_kev", Type::F32, {un}, raw(er.data(), 4 * n)});
+        w.add_dataset({"int_type", Type::I8, {un}, raw(int_type.data(), n)});
+        w.add_dataset({"n_int", Type::I16, {un}, raw(n_int.data(), 2 * n)});
+        w.add_attribute(attr_str("tag", g.tag));
+        w.add_attribute(attr_num("n_events", Type::I64, (int64_t)n));
+        w.add_attribute(attr_num("seed", Type::I64, (int64_t)g.seed));
+        w.add_attribute(attr_str("crystal", g.crystal_name));
+        w.add_attribute(attr_num("pde", Type::F32, g.op.pde));
+        w.add_attribute(attr_str("backend", "cuda"));
+        w.add_attribute(attr_str("int_type_key", INT_TYPE_KEY));
+        w.add_attribute(attr_str("tmin_nohit", "Inf"));
+        make_dirs(g.outdir);
+        copy_file(g.cfg_path, join(g.outdir, basename_of(g.cfg_path)));
+        w.write(join(g.outdir, "events.h5"));
+    }
+    // summary, scripts/shoot_gammas.jl:80-90
+    int64_t inter = 0;
+    std::vector<double> pe;
+    for (int64_t i = 0; i < n; ++i) {
+        inter += edep[i] > 0.0f;
+        if (edep[i] > 510.0f) pe.push_back((double)npe[i]);
+    }
+    const double nn = (double)std::max<int64_t>(n, 1);
+    std::printf("%-14s %lld events (%.1fs, cuda): interacted %.1f%%, photopeak %.1f%%\n", g.tag.c_str(),
+                (long long)n, elapsed, 100.0 * inter / nn, 100.0 * pe.size() / nn);
+    if (pe.size() > 1) {
+        double mean = 0.0, var = 0.0;
+        for (double v : pe) mean += v;
+        mean /= pe.size();
+        for (double v : pe) var += (v - mean) * (v - mean);
+        const double sd = std::sqrt(var / (pe.size() - 1));
+        std::printf("%-14s photopeak: %.0f pe mean, FWHM/mean %.2f%% (photostatistics+transport only)\n", "",
+                    mean, 235.5 * sd / mean);
+    }
+    std::fflush(stdout);
+    return 0;
+}
+
+// One run file: a point source or a gamma campaign.
+struct Job {
+    bool gamma = false;
+    Setup point;
+    GammaSetup campaign;
+};
+
 void usage()
 {
     std::fprintf(stderr,
                  "usage: crysplight_run [--device N] [--data DIR] [--output-root DIR] [--n-photons N]\n"
-                 "                      [--print-setup] [--no-write] run.toml ...\n");
+                 "                      [--n-events N] [--print-setup] [--no-write] run.toml ...\n");
 }
 
 }  // namespace
@@ -366,7 +618,7 @@ int main(int argc, char** argv)
 {
     int device = 0;
     std::string data_dir, out_root;
-    int64_t n_override = -1;
+    int64_t n_override = -1, ev_override = -1;
     bool print_only = false, write = true;
     std::vector<std::string> files;
     for (int i = 1; i < argc; ++i) {
@@ -391,6 +643,7 @@ int main(int argc, char** argv)
         else if (a == "--data") data_dir = arg("--data");
         else if (a == "--output-root") out_root = arg("--output-root");
         else if (a == "--n-photons") n_override = count("--n-photons");
+        else if (a == "--n-events") ev_override = count("--n-events");
         else if (a == "--print-setup") print_only = true;
         else if (a == "--no-write") write = false;
         else if (a == "-h" || a == "--help") { usage(); return 0; }
@@ -398,18 +651,29 @@ int main(int argc, char** argv)
         else files.push_back(a);
     }
     if (files.empty()) { usage(); return 2; }
-    std::vector<Setup> setups;
+    std::vector<Job> jobs;
     try {
         for (const std::string& f : files) {
-            setups.push_back(load_setup(f, data_dir, out_root));
-            if (n_override >= 0) setups.back().n_photons = n_override;
+            Job j;
+            j.gamma = cltoml::parse_file(absolute(f)).count("campaign") != 0;
+            if (j.gamma) {
+                j.campaign = load_gamma_setup(f, data_dir, out_root);
+                if (ev_override >= 0) j.campaign.n_events = ev_override;
+            } else {
+                j.point = load_setup(f, data_dir, out_root);
+                if (n_override >= 0) j.point.n_photons = n_override;
+            }
+            jobs.push_back(std::move(j));
         }
     } catch (const std::exception& e) {
         std::fprintf(stderr, "crysplight_run: %s\n", e.what());
         return 1;
     }
     if (print_only) {
-        for (const Setup& s : setups) print_setup(s);
+        for (const Job& j : jobs) {
+            if (j.gamma) print_gamma_setup(j.campaign);
+            else print_setup(j.point);
+        }
         return 0;
     }
     cl_handle* h = nullptr;
@@ -419,7 +683,7 @@ int main(int argc, char** argv)
     }
     int rc = 0;
     try {
-        for (const Setup& s : setups) rc |= run_one(h, s, write);
+        for (const Job& j : jobs) rc |= j.gamma ? run_gamma(h, j.campaign, write) : run_one(h, j.point, write);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "crysplight_run: %s\n", e.what());
         rc = 1;

@@ -26,9 +26,16 @@ int main(int argc, char** argv)
         std::memcpy(f.raw.data() + 4 * k, &v, 4);
     }
     Dataset e{"empty", Type::F64, {0}, Bytes()};
+    // small integer types of events.h5: int8 (2, 3), int16 (3,), uint16 (3,)
+    Dataset i8{"int_type", Type::I8, {2, 3}, Bytes{0xFF, 0, 1, 2, 0x80, 0x7F}};
+    Dataset i16{"n_int", Type::I16, {3}, Bytes{0xFF, 0xFF, 0x02, 0x00, 0x00, 0x80}};
+    Dataset u16{"maps", Type::U16, {3}, Bytes{0x01, 0x00, 0xFF, 0xFF, 0x34, 0x12}};
     w.add_dataset(c);
     w.add_dataset(f);
     w.add_dataset(e);
+    w.add_dataset(i8);
+    w.add_dataset(i16);
+    w.add_dataset(u16);
     w.add_attribute(attr_str("tag", "h5 check"));
     w.add_attribute(attr_num("n_photons", Type::I64, (int64_t)1000000));
     w.add_attribute(attr_num("bin_ns", Type::F32, 100.0f));

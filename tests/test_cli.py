@@ -11,11 +11,14 @@ import numpy as np
 import pytest
 
 from crysplight_b200.config import load_setup
+from crysplight_b200.shoot_gammas import load_gamma_setup
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "crysplight_b200")
 CLI = os.path.join(PKG, "lib", "crysplight_run")
 RUNS = [os.path.join(PKG, "runs", f) for f in ("point_csitl_teflon.toml", "point_bgo_esr.toml")]
+GAMMA_RUNS = [os.path.join(PKG, "runs", f) for f in ("gammas_csitl_50k.toml", "gammas_bgo_500k.toml",
+                                                      "gammas_bgo_esr_500k.toml")]
 
 
 @pytest.fixture(scope="module")
@@ -95,6 +98,25 @@ dir = "elsewhere"
 """
 
 
+@pytest.mark.parametrize("path", GAMMA_RUNS)
+def test_gamma_campaign_setup_matches_the_python_mirror(cli, path):
+    j = _setup_json(cli, path)
+    st = load_gamma_setup(path)
+    f32 = np.float32
+    assert j["tag"] == st.tag and os.path.realpath(j["outdir"]) == os.path.realpath(st.outdir)
+    assert [f32(v) for v in j["box"]] == [f32(v) for v in st.box.L]
+    for k in ("n_crystal", "n_coupling", "abs_len_mm", "rayleigh_mm", "wrap_R", "sigma_alpha", "pde"):
+        assert f32(j["op"][k]) == f32(getattr(st.op, k)), k
+    assert j["op"]["wrap_specular"] == st.op.wrap_specular and j["op"]["air_gap"] == st.op.air_gap
+    assert f32(j["grid"][0]) == f32(st.ro.grid.pitch_mm) and j["grid"][1:] == [st.ro.grid.nx, st.ro.grid.ny]
+    assert f32(j["tb"][0]) == f32(st.tb.bin_ns) and j["tb"][1] == st.tb.nbins
+    assert j["yield_per_mev"] == st.yield_per_mev and f32(j["tau_ns"]) == f32(st.tau_ns)
+    assert (j["n_events"], j["seed"]) == (st.n_events, st.seed)
+    assert j["crystal"] == st.cfg["crystal"]["material"] and j["density"] == st.density
+    assert os.path.realpath(j["xcom"]) == os.path.realpath(st.xcom_path)
+    assert _setup_json(cli, path, "--n-events", "7")["n_events"] == 7
+
+
 def test_toml_subset_edge_cases(cli, tmp_path):
     runs = tmp_path / "runs"
     runs.mkdir()
@@ -159,7 +181,10 @@ def test_hdf5_writer_matches_the_python_writer(tmp_path):
     ff[4] = np.inf
     first = ff.reshape((3, 2), order="F")
     out_p = tmp_path / "p.h5"
-    write_h5(str(out_p), {"counts": counts, "first_time_ns": first, "empty": np.zeros(0, np.float64)},
+    i8 = np.array([-1, 0, 1, 2, -128, 127], np.int8).reshape((2, 3), order="F")
+    write_h5(str(out_p), {"counts": counts, "first_time_ns": first, "empty": np.zeros(0, np.float64),
+                          "int_type": i8, "n_int": np.array([-1, 2, -32768], np.int16),
+                          "maps": np.array([1, 65535, 0x1234], np.uint16)},
              {"tag": "h5 check", "n_photons": np.int64(1000000), "bin_ns": np.float32(100.0),
               "nbins": np.int32(80), "flag": np.uint8(1), "big": np.uint64(0xFFFFFFFFFFFFFFF0),
               "u32": np.uint32(4000000000), "sigma_alpha_deg": np.float64(1.3), "empty_str": ""})
@@ -167,6 +192,31 @@ def test_hdf5_writer_matches_the_python_writer(tmp_path):
     d, a = read_h5(str(out_c))
     assert np.array_equal(d["counts"], counts) and a["tag"] == "h5 check"
     assert np.array_equal(d["first_time_ns"], first)
+
+
+@pytest.mark.gpu
+def test_cli_gamma_campaign_writes_the_same_events_h5_as_python(cli, tmp_path):
+    """A gamma campaign through crysplight_run and through shoot_gammas: the
+    two events.h5 files are identical byte for byte."""
+    from crysplight_b200.shoot_gammas import shoot_gammas
+    from crysplight_b200.transport import Engine
+    runs = tmp_path / "runs"
+    runs.mkdir()
+    for src in GAMMA_RUNS[:2]:
+        p = runs / os.path.basename(src)
+        p.write_text(open(src).read())
+        eng = Engine(0)
+        try:
+            shoot_gammas(str(p), engine=eng, n_events=400)
+        finally:
+            eng.close()
+        tag = load_gamma_setup(str(p)).tag
+        py_file = tmp_path / "output" / tag / "events.h5"
+        shutil.move(str(py_file), str(tmp_path / f"{tag}.py.h5"))
+        r = subprocess.run([cli, "--n-events", "400", str(p)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        assert "events" in r.stdout and "interacted" in r.stdout
+        assert (tmp_path / f"{tag}.py.h5").read_bytes() == py_file.read_bytes()
 
 
 @pytest.mark.gpu
