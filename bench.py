@@ -51,14 +51,13 @@ import numpy as np
 # instrumented oracle (python -m oracle.opcount).
 OPS_PER_STEP = {"scan256": 165.6, "point1m": 186.7}
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (read + write) per launch of the transport kernel: one ncu capture
-# of the scan at 20,000 photons per point (profiles/transport_kernel_scan256x20k.md,
-# 3.00 GB for 494.8M photon-steps) scaled to the full launch by photon-steps.
-# Almost all of it is L2 misses of the 64 MB log table (about 2 bytes per
-# photon-step x log lookup), which grow in proportion to the steps; the
-# sources, offsets and maps are 0.24 MB.  point1m: not captured.
-TRAFFIC_PER_STEP = (2.993991e9 + 6.48064e6) / 494_804_727
-TRAFFIC_BYTES = {"point1m": None}
+# DRAM bytes (read + write) per photon-step of the transport kernel, from one
+# ncu capture of each workload at a reduced size (scan: 20,000 photons per
+# point, 3.00 GB for 494.8M photon-steps), scaled to a full launch by its
+# photon-steps.  Almost all of it is L2 misses of the 64 MB log table (about 2
+# bytes per photon-step and lookup), which grow in proportion to the steps;
+# the sources, offsets and maps are 0.24 MB.
+TRAFFIC_PER_STEP = {"scan256": (2.993991e9 + 6.48064e6) / 494_804_727, "point1m": None}
 # Warp instructions the transport kernel issues per photon-step (smsp__inst_executed
 # of the same ncu capture: 17.23 G for 494.8M photon-steps); with the live
 # steps/s this gives the kernel's issue rate against the SMs' issue slots.
@@ -79,7 +78,8 @@ def events_workload(n_events: int = 50_000):
                 desc=f"{n_events} 511 keV gammas, CsI(Tl)+Teflon 48x48x37.2 mm, PDE 0.40")
 
 
-def run_events_bench(eng, E, steps: int, warmup: int, dev, stream, pid_base: int = 0):
+def run_events_bench(eng, E, steps: int, warmup: int, dev, stream, pid_base: int = 0,
+                     tune_events: int = 0):
     """events/s: the transport of all events' photons with the deposits in HBM
     (value: one CUDA-graph replay of init + transport + finalize per step, at
     the launch shape the autotuner picked), and the whole public pipeline
@@ -95,7 +95,17 @@ def run_events_bench(eng, E, steps: int, warmup: int, dev, stream, pid_base: int
     ev = DeviceEvents(eng, E["box"], E["op"], E["ro"], E["tb"], xyz=T(g.dep_xyz), t0=T(g.dep_t),
                       photons=T(g.dep_photons), segment=T(g.dep_event), n_segments=n_seg,
                       seed=E["seed"], tau_ns=E["tau"], pid_offset=pid_base)
-    best, tune_times = autotune(eng, ev.step, stream=stream, repeats=2)
+    if tune_events and tune_events < E["n_events"]:
+        # the launch shape is timed on the first tune_events events (same photons and streams)
+        k = int(np.searchsorted(g.dep_event, tune_events, side="left"))
+        ev_t = DeviceEvents(eng, E["box"], E["op"], E["ro"], E["tb"], xyz=T(g.dep_xyz[:k]),
+                            t0=T(g.dep_t[:k]), photons=T(g.dep_photons[:k]),
+                            segment=T(g.dep_event[:k]), n_segments=tune_events, seed=E["seed"],
+                            tau_ns=E["tau"], pid_offset=pid_base)
+        best, tune_times = autotune(eng, ev_t.step, stream=stream, repeats=2)
+        del ev_t
+    else:
+        best, tune_times = autotune(eng, ev.step, stream=stream, repeats=2)
     ev.capture()
     for _ in range(warmup):
         ev.replay()
@@ -260,7 +270,11 @@ def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wal
         ne = int(np.count_nonzero((g.dep_xyz[:, 2] >= z0 + se.expert_margin_mm) & (g.dep_xyz[:, 2] <= z1)))
         launches += (2 + len(e.members) * chunks(ne) * 4) if ne else 0
     se.close()
+    # the rule's ceiling: with the surrogate free, only the sites within the
+    # wall margin would still go through the Monte Carlo
+    ceiling = stats["photons_total"] / max(stats["photons_wall"], 1)
     return dict(value=n_seg / dev_s, e2e=n_seg / e2e_s, dev_s=dev_s, mc_value=n_seg / mc_s,
+                ceiling_speedup=ceiling,
                 mc_s=mc_s, mc_photon_steps=mc_steps, photons=int(off[-1]), deposits=nd,
                 members=len(sur.members), experts=len(experts), launches=launches,
                 stats=stats, photopeak_surrogate=pk_s, photopeak_mc=pk_m,
@@ -385,62 +399,76 @@ def measured_peaks() -> dict:
 # ------------------------------------------------------------------------------------
 # reference arm / CPU baseline: the oracle on the host cores
 # ------------------------------------------------------------------------------------
-def cpu_run(W, n_points: int, per_point: int) -> tuple[float, int]:
+def cpu_run(W, per_point: int) -> tuple[float, int, int]:
+    """The oracle on all host threads over every point of the workload with
+    ``per_point`` photons each: (seconds, photons, photon-steps)."""
     from oracle import oracle
-    pts = W["points"][:n_points]
+    pts = W["points"]
+    n_points = pts.shape[0]
     t0 = time.perf_counter()
     if W["name"] == "scan256":
-        oracle.run_segments(W["box"], W["op"], W["ro"], W["tb"], sources=pts,
-                            photons_per_source=[per_point] * n_points,
-                            segment_of_source=range(n_points), n_segments=n_points,
-                            seed=W["seed"], tau_ns=W["tau"], nthreads=os.cpu_count())
+        _, steps = oracle.run_segments(W["box"], W["op"], W["ro"], W["tb"], sources=pts,
+                                       photons_per_source=[per_point] * n_points,
+                                       segment_of_source=range(n_points), n_segments=n_points,
+                                       seed=W["seed"], tau_ns=W["tau"], nthreads=os.cpu_count(),
+                                       return_steps=True)
     else:
-        oracle.run_photons(W["box"], W["op"], W["ro"], W["tb"], n_photons=per_point,
-                           seed=W["seed"], pos=tuple(pts[0]), tau_ns=W["tau"],
-                           nthreads=os.cpu_count())
+        _, steps = oracle.run_photons_ka(W["box"], W["op"], W["ro"], W["tb"], n_photons=per_point,
+                                         seed=W["seed"], pos=tuple(pts[0]), tau_ns=W["tau"],
+                                         nthreads=os.cpu_count(), return_steps=True)
     dt = time.perf_counter() - t0
-    return dt, n_points * per_point
+    return dt, n_points * per_point, int(steps)
 
 
-def cpu_sample_size(W, target_s: float) -> tuple[int, int]:
-    """(points, photons per point) of a sample that takes about target_s."""
-    if W["name"] == "scan256":
-        dt, n = cpu_run(W, 1, 20_000)
-        pts = int(max(1, min(256, target_s / (dt * W["per_point"] / 20_000))))
-        return pts, W["per_point"]
-    dt, n = cpu_run(W, 1, 50_000)
-    per = int(max(50_000, min(W["per_point"] * 50, target_s / dt * 50_000)))
-    return 1, per
+def cpu_sample_size(W, target_s: float) -> int:
+    """Photons per point of a sample over all the workload's points (the same
+    points, optics and seed) that takes about target_s on the host."""
+    probe = 2_000 if W["name"] == "scan256" else 20_000
+    dt, _, _ = cpu_run(W, probe)
+    per = int(probe * target_s / max(dt, 1e-3))
+    return int(max(probe, min(W["per_point"], per)))
+
+
+def cpu_sample_desc(W, per: int, dt: float) -> str:
+    pts = W["points"].shape[0]
+    return (f"all {pts} point(s) of the {W['name']} workload x {per} photons "
+            f"({dt:.1f} s on {os.cpu_count()} threads)")
 
 
 def cpu_baseline(W, target_s: float) -> dict:
-    pts, per = cpu_sample_size(W, target_s)
-    dt, n = cpu_run(W, pts, per)
+    per = cpu_sample_size(W, target_s)
+    dt, n, steps = cpu_run(W, per)
     return {"value": n / dt, "unit": "photons/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{pts} point(s) x {per} photons of the {W['name']} workload "
-                      f"({dt:.1f} s on {os.cpu_count()} threads)"}
+            "photon_steps_per_s": steps / dt, "sample": cpu_sample_desc(W, per, dt)}
+
+
+def workload_config(W) -> dict:
+    """The workload the line is quoted on (the same dict in both arms)."""
+    return {"workload": W["name"], "desc": W["desc"], "photons_per_step": W["n"]}
 
 
 def run_reference_arm(args, W, rank, world):
     if rank != 0:
         return
-    pts, per = cpu_sample_size(W, args.cpu_seconds)
+    per = cpu_sample_size(W, args.cpu_seconds)
     for _ in range(args.warmup):
-        cpu_run(W, pts, per)
-    times = []
+        cpu_run(W, per)
+    times, tot_n, tot_steps = [], 0, 0
     for _ in range(args.steps):
-        dt, n = cpu_run(W, pts, per)
+        dt, n, st = cpu_run(W, per)
         times.append(dt)
-    tot_n = n * args.steps
+        tot_n += n
+        tot_steps += st
     value = tot_n / sum(times)
-    sample = (f"{pts} point(s) x {per} photons of the {W['name']} workload per step "
-              f"(C restatement of the reference CPU transport, {os.cpu_count()} threads)")
+    sample = cpu_sample_desc(W, per, sum(times) / len(times)) + \
+        " per step (C restatement of the reference CPU transport)"
     line = {
         "impl": "reference", "metric": "photons/s", "value": value, "unit": "photons/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * sum(times) / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": W["name"], "desc": W["desc"], "sample_photons_per_step": n},
+        "config": workload_config(W),
+        "photon_steps_per_s": tot_steps / sum(times),
         "cpu_baseline": {"value": value, "unit": "photons/s", "cores": os.cpu_count(),
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0,
@@ -452,20 +480,13 @@ def run_reference_arm(args, W, rank, world):
 # ------------------------------------------------------------------------------------
 # CUDA arm
 # ------------------------------------------------------------------------------------
-def run_cuda_arm(args, W, rank, world, local_rank):
+def measure_photons(eng, W, steps: int, warmup: int, dev, stream, pid_base: int = 0,
+                    clocks: bool = True) -> dict:
+    """photons/s of one workload: ``value`` with the inputs resident in HBM
+    (device entry point, CUDA events on the launch stream, L2 flushed between
+    steps) and ``e2e`` through the host-buffer C-ABI call (pinned host inputs
+    copied in, maps / times / counters copied out), timed by the host clock."""
     import torch
-    import crysplight_b200 as cl
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    eng = cl.Engine(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-
-    pid_base = rank * W["n"]        # disjoint photon ids per rank
-    stream = torch.cuda.Stream(dev)  # explicit stream: the library launches on it
-    torch.cuda.set_stream(stream)
-    sptr = stream.cuda_stream
     nx = ny = 8
     pts = W["points"]
     npts = pts.shape[0]
@@ -473,15 +494,14 @@ def run_cuda_arm(args, W, rank, world, local_rank):
         off = np.zeros(npts + 1, np.int64)
         off[1:] = np.cumsum(np.full(npts, W["per_point"], np.int64))
         seg = np.arange(npts, dtype=np.int32)
-        d_sx = torch.from_numpy(np.ascontiguousarray(pts[:, 0])).to(dev)
-        d_sy = torch.from_numpy(np.ascontiguousarray(pts[:, 1])).to(dev)
-        d_sz = torch.from_numpy(np.ascontiguousarray(pts[:, 2])).to(dev)
+        d_sx, d_sy, d_sz = (torch.from_numpy(np.ascontiguousarray(pts[:, i])).to(dev) for i in range(3))
         d_off = torch.from_numpy(off).to(dev)
         d_seg = torch.from_numpy(seg).to(dev)
         d_maps = torch.empty(nx * ny * npts, dtype=torch.int32, device=dev)
         d_tmin = torch.empty(nx * ny * npts, dtype=torch.float32, device=dev)
         d_npe = torch.empty(npts, dtype=torch.int32, device=dev)
         d_ctr = torch.empty(9, dtype=torch.int64, device=dev)
+        sptr = stream.cuda_stream
 
         def device_step():
             eng.run_segments_device(
@@ -492,7 +512,6 @@ def run_cuda_arm(args, W, rank, world, local_rank):
                 tmin=d_tmin.data_ptr(), npe=d_npe.data_ptr(), counters=d_ctr.data_ptr(),
                 stream=sptr)
 
-        # pinned host inputs for the end-to-end path
         h_pts = torch.from_numpy(np.ascontiguousarray(pts)).pin_memory().numpy()
         h_cnt = torch.full((npts,), W["per_point"], dtype=torch.int64).pin_memory().numpy()
         h_seg = torch.from_numpy(seg).pin_memory().numpy()
@@ -504,6 +523,7 @@ def run_cuda_arm(args, W, rank, world, local_rank):
                                     tau_ns=W["tau"])
         h2d = 3 * 4 * npts + 8 * (npts + 1) + 4 * npts
         d2h = 2 * 4 * nx * ny * npts + 4 * npts + 72 + 12
+        in_bytes = 3 * 4 * npts + 8 * (npts + 1) + 4 * npts
         out_bytes = 2 * 4 * nx * ny * npts + 4 * npts + 72
         launches = 3
     else:
@@ -512,6 +532,7 @@ def run_cuda_arm(args, W, rank, world, local_rank):
         d_counts = torch.empty(nx * ny * nb, dtype=torch.int32, device=dev)
         d_first = torch.empty(nx * ny, dtype=torch.float32, device=dev)
         d_ctr = torch.empty(9, dtype=torch.int64, device=dev)
+        sptr = stream.cuda_stream
 
         def device_step():
             eng.run_photons_device(W["box"], W["op"], W["ro"], W["tb"], px=d_p[0].data_ptr(),
@@ -528,112 +549,139 @@ def run_cuda_arm(args, W, rank, world, local_rank):
                                       tau_ns=W["tau"])
         h2d = 3 * 4
         d2h = 4 * nx * ny * nb + 4 * nx * ny + 72 + 12
+        in_bytes = 3 * 4
         out_bytes = 4 * nx * ny * nb + 4 * nx * ny + 72
         launches = 2
 
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
-
-    def barrier():
-        torch.cuda.synchronize(dev)
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-
-    # warm-up
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         device_step()
     eng.sync(sptr)
     host_step()
 
-    # ---- device-resident timing ----
-    clocks = ClockSampler(local_rank)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    barrier()
-    clocks.start()
+    clk = ClockSampler(dev.index or 0) if clocks else None
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    torch.cuda.synchronize(dev)
+    if clk:
+        clk.start()
     t_wall0 = time.perf_counter()
-    for i in range(args.steps):
+    for i in range(steps):
         flush.zero_()                       # evict L2 between timed steps
         starts[i].record(stream)
         device_step()
         stops[i].record(stream)
     eng.sync(sptr)
-    barrier()
+    torch.cuda.synchronize(dev)
     t_wall = time.perf_counter() - t_wall0
-    clk = clocks.stop()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    clk_rec = clk.stop() if clk else None
+    tot_ms = sum(s.elapsed_time(e) for s, e in zip(starts, stops))
     steps_per_launch = eng.last_steps
-    tot_ms = sum(step_ms)
 
-    # ---- end-to-end through the host-buffer C-ABI ----
-    barrier()
+    torch.cuda.synchronize(dev)
     e2e_t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         host_step()
-    barrier()
+    torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - e2e_t0
+    return dict(tot_ms=tot_ms, e2e_s=e2e_s, steps_per_launch=steps_per_launch, h2d=h2d, d2h=d2h,
+                in_bytes=in_bytes, out_bytes=out_bytes, launches=launches, clocks=clk_rec,
+                wall_s=t_wall)
 
-    if dist is not None:
-        t = torch.tensor([tot_ms, e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms, e2e_s = float(t[0]), float(t[1])
 
-    if rank != 0:
-        eng.close()
-        return
-    n_total = W["n"] * args.steps * world
-    value = n_total / (tot_ms * 1e-3)
-    e2e_value = n_total / e2e_s
+def roofline(W, steps_per_launch: int, launch_s: float, in_bytes: int, out_bytes: int, n_sm: int) -> dict:
+    """The transport kernel against the SMs' lane-op ceiling (its bound), its
+    issue rate against the issue slots, and its DRAM traffic (the L2 misses of
+    the 64 MB log table dominate it) against HBM."""
     peaks = measured_peaks()
-    props = torch.cuda.get_device_properties(dev)
-    n_sm = props.multi_processor_count
-    launch_s = tot_ms * 1e-3 / args.steps
+    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
     ops_step = OPS_PER_STEP[W["name"]]
     achieved = ops_step * steps_per_launch / launch_s
-    peak = n_sm * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6
-    line = {
-        "metric": "photons/s", "value": value, "unit": "photons/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": W["name"], "desc": W["desc"], "photons_per_step_per_gpu": W["n"],
-                   "l2": "flushed between timed steps (256 MiB memset)",
-                   "parallelism": f"photon-range shards x{world}"},
-        "e2e": {"value": e2e_value, "unit": "photons/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches * args.steps,
-        "photon_steps_per_launch": steps_per_launch,
-        "photon_steps_per_s": steps_per_launch / launch_s,
-        "roofline": {
-            "bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gop/s",
-            "frac": achieved / peak,
-            "traffic": (TRAFFIC_PER_STEP * steps_per_launch if W["name"] == "scan256"
-                        else TRAFFIC_BYTES.get(W["name"])),
-            "ops_per_step": ops_step,
-            "note": ("reference Float32/int ops per photon-step x steps / launch time, against "
-                     "one op per lane per clock (SMs x 128 lanes x max SM clock of measured)"),
-            "hbm": {"achieved": out_bytes / launch_s / 1e9, "peak": peaks.get("hbm_gbs"),
-                    "unit": "GB/s", "frac": out_bytes / launch_s / 1e9 / peaks.get("hbm_gbs", 1)},
-            "issue_slots": issue_slots(W["name"], steps_per_launch / launch_s, n_sm,
-                                       peaks.get("sm_max_mhz", 1965.0)),
-        },
-        "clocks": clk,
-        "wall_s_timed": t_wall,
+    peak = n_sm * 128 * sm_mhz * 1e6
+    tps = TRAFFIC_PER_STEP.get(W["name"])
+    traffic = tps * steps_per_launch if tps else None
+    hbm_peak = peaks.get("hbm_gbs", 6553.3)
+    dram = traffic if traffic is not None else float(in_bytes + out_bytes)
+    return {
+        "bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gop/s",
+        "frac": achieved / peak, "traffic": traffic, "ops_per_step": ops_step,
+        "note": ("reference Float32/int ops per photon-step x steps / launch time, against "
+                 "one op per lane per clock (SMs x 128 lanes x max SM clock of measured)"),
+        "hbm": {"achieved": dram / launch_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": dram / launch_s / 1e9 / hbm_peak, "dram_bytes": dram,
+                "algorithmic_bytes": in_bytes + out_bytes,
+                "note": ("DRAM bytes per launch (ncu dram__bytes read+write per photon-step x "
+                         "steps: L2 misses of the log table) over the launch time; the "
+                         "algorithmic bytes are the sources, offsets, maps, times and counters")},
+        "issue_slots": issue_slots(W["name"], steps_per_launch / launch_s, n_sm, sm_mhz),
     }
-    if world == 1 and not args.no_cpu_baseline:
+
+
+def run_cuda_arm(args, W, rank, world, local_rank):
+    import torch
+    import crysplight_b200 as cl
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        run_sharded_arm(args, W, rank, world, local_rank)
+        return
+    eng = cl.Engine(local_rank)
+    stream = torch.cuda.Stream(dev)  # explicit stream: the library launches on it
+    torch.cuda.set_stream(stream)
+    r = measure_photons(eng, W, args.steps, args.warmup, dev, stream)
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    launch_s = r["tot_ms"] * 1e-3 / args.steps
+    n_total = W["n"] * args.steps
+    line = {
+        "metric": "photons/s", "value": n_total / (r["tot_ms"] * 1e-3), "unit": "photons/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["tot_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(W),
+        "l2": "flushed between timed steps (256 MiB memset)", "parallelism": "1 GPU",
+        "e2e": {"value": n_total / r["e2e_s"], "unit": "photons/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"]},
+        "gpu_launches": r["launches"] * args.steps,
+        "photon_steps_per_launch": r["steps_per_launch"],
+        "photon_steps_per_s": r["steps_per_launch"] / launch_s,
+        "roofline": roofline(W, r["steps_per_launch"], launch_s, r["in_bytes"], r["out_bytes"], n_sm),
+        "clocks": r["clocks"],
+        "wall_s_timed": r["wall_s"],
+    }
+    if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(W, args.cpu_seconds)
-    if world == 1 and args.events > 0:
-        # secondary metric: 511 keV events/s of the event pipeline (10,000 CsI(Tl) events)
+    if W["name"] == "scan256" and args.point1m:
+        # config 1 at its stated size: 10^6 CsI(Tl)+Teflon photons from the centre
+        P = workload("point1m")
+        rp = measure_photons(eng, P, max(args.steps, 10), args.warmup, dev, stream)
+        ls = rp["tot_ms"] * 1e-3 / max(args.steps, 10)
+        obj = {"metric": "photons/s", "workload": P["desc"], "unit": "photons/s",
+               "value": P["n"] / ls, "e2e": {"value": P["n"] * max(args.steps, 10) / rp["e2e_s"],
+                                             "unit": "photons/s", "h2d_bytes_per_step": rp["h2d"],
+                                             "d2h_bytes_per_step": rp["d2h"]},
+               "ms_per_step": ls * 1e3, "photon_steps_per_launch": rp["steps_per_launch"],
+               "photon_steps_per_s": rp["steps_per_launch"] / ls,
+               "roofline": roofline(P, rp["steps_per_launch"], ls, rp["in_bytes"], rp["out_bytes"], n_sm),
+               "clocks": rp["clocks"]}
+        if not args.no_cpu_baseline:
+            obj["cpu_baseline"] = cpu_baseline(P, args.cpu_seconds)
+        line["point1m"] = obj
+    if args.events > 0:
+        # 511 keV events/s of the event pipeline (runs/gammas_csitl_50k.toml: 50,000 events)
         E = events_workload(args.events)
-        r = run_events_bench(eng, E, args.steps, args.warmup, dev, stream)
-        line["events"] = {"metric": "511keV events/s", "workload": E["desc"],
-                          "value": r["value"], "e2e": r["e2e"], "unit": "events/s",
-                          "photons_per_event": r["photons"] / E["n_events"],
-                          "photon_steps_per_s": r["photon_steps"] / r["dev_s"],
-                          "launch": r["launch"], "cuda_graph": True}
-    if world == 1 and args.surrogate_training:
+        r = run_events_bench(eng, E, args.steps, args.warmup, dev, stream,
+                             tune_events=args.tune_events)
+        obj = {"metric": "511keV events/s", "workload": E["desc"],
+               "value": r["value"], "e2e": r["e2e"], "unit": "events/s",
+               "photons_per_event": r["photons"] / E["n_events"],
+               "photon_steps_per_s": r["photon_steps"] / r["dev_s"],
+               "launch": r["launch"], "cuda_graph": True}
+        if not args.no_cpu_baseline:
+            obj["cpu_baseline"] = events_cpu_baseline(E, args.cpu_seconds)
+        line["events"] = obj
+    if args.surrogate_training:
         line["surrogate_training"] = surrogate_training_bench(dev)
-    if world == 1 and args.surrogate_events > 0 and os.path.exists(SURROGATE_BGO):
+    if args.surrogate_events > 0 and os.path.exists(SURROGATE_BGO):
         # secondary metric: 500,000 BGO+ESR events, surrogate + Monte Carlo fallback vs
         # the plain Monte Carlo
         E = surrogate_events_workload(args.surrogate_events)
@@ -643,10 +691,102 @@ def run_cuda_arm(args, W, rank, world, local_rank):
             "metric": "511keV events/s", "workload": E["desc"], "unit": "events/s",
             "value": r["value"], "e2e": r["e2e"], "plain_mc": r["mc_value"],
             "speedup_vs_plain_mc": r["value"] / r["mc_value"],
+            "ceiling_speedup": r["ceiling_speedup"],
             "photopeak_shift": r["photopeak_shift"], "maps_vs_mc": r["maps"],
             "fallback_sites": r["stats"]["fallback_sites"], "sites": r["stats"]["sites"],
             "readout_face_expert": bool(r["experts"])}
     print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def run_sharded_arm(args, W, rank, world, local_rank):
+    """N GPUs, one process each, on the product's multi-GPU path: one job of
+    N copies of the workload's points (N x 256 segments, photon ids numbered
+    over the whole job), split by whole segments over the ranks
+    (sharding.ShardedSegments: each rank transports its share from HBM, then
+    NCCL all_gather of every rank's maps / times / npe and all_reduce of the
+    counters); the time of a step is the max over ranks of transport + gather.
+    e2e: the same job through sharding.run_segments_sharded with host buffers."""
+    import torch
+    import torch.distributed as dist
+    import crysplight_b200 as cl
+    from crysplight_b200.sharding import ShardedSegments, run_segments_sharded
+    if W["name"] != "scan256":
+        raise SystemExit("--gpus N > 1 runs the scan256 workload")
+    dev = torch.device("cuda", local_rank)
+    eng = cl.Engine(local_rank)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    pts = np.tile(W["points"], (world, 1))
+    nseg = pts.shape[0]
+    cnt = np.full(nseg, W["per_point"], np.int64)
+    seg = np.arange(nseg, dtype=np.int64)
+    job = ShardedSegments(eng, W["box"], W["op"], W["ro"], W["tb"], sources=pts, photons_per_source=cnt,
+                          segment_of_source=seg, n_segments=nseg, seed=W["seed"], tau_ns=W["tau"])
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        job.step()
+    job.sync()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        job.step()
+        stops[i].record(stream)
+    job.sync()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    clk = clocks.stop()
+    tot_ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops))
+    steps_local = eng.last_steps
+    # end to end: host buffers through run_segments_sharded (copies, gather via NCCL)
+    runner = lambda **kw: eng.run_segments(W["box"], W["op"], W["ro"], W["tb"], seed=W["seed"],
+                                           tau_ns=W["tau"], **kw)
+    run_segments_sharded(runner, sources=pts, photons_per_source=cnt, segment_of_source=seg,
+                         n_segments=nseg)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        run_segments_sharded(runner, sources=pts, photons_per_source=cnt, segment_of_source=seg,
+                             n_segments=nseg)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([tot_ms, e2e_s, float(steps_local)], dtype=torch.float64, device=dev)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = t.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    job = None
+    if rank == 0:
+        tot_ms, e2e_s = float(mx[0]), float(mx[1])
+        n_total = int(cnt.sum()) * args.steps
+        launch_s = tot_ms * 1e-3 / args.steps
+        line = {
+            "metric": "photons/s", "value": n_total / (tot_ms * 1e-3), "unit": "photons/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(W),
+            "job": f"{world} x {W['points'].shape[0]} points x {W['per_point']} photons, "
+                   "whole-segment shards, NCCL all_gather of the maps",
+            "l2": "flushed between timed steps (256 MiB memset)",
+            "parallelism": f"segment shards x{world} (sharding.ShardedSegments)",
+            "e2e": {"value": n_total / e2e_s, "unit": "photons/s",
+                    "h2d_bytes_per_step": int(3 * 4 * nseg + 8 * (nseg + 1) + 4 * nseg),
+                    "d2h_bytes_per_step": int(2 * 4 * 64 * nseg + 4 * nseg + 72)},
+            "gpu_launches": 3 * args.steps,
+            "photon_steps_per_s": float(sm[2]) / launch_s,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
     eng.close()
 
 
@@ -675,7 +815,8 @@ def run_events_arm(args, rank, world, local_rank):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     eng = cl.Engine(local_rank)
-    r = run_events_bench(eng, E, args.steps, args.warmup, dev, stream, pid_base=0)
+    r = run_events_bench(eng, E, args.steps, args.warmup, dev, stream, pid_base=0,
+                         tune_events=args.tune_events)
     dev_s, e2e_s = r["dev_s"], r["e2e_s"]
     if world > 1:
         import torch.distributed as dist
@@ -778,9 +919,14 @@ def main():
     ap.add_argument("--workload", choices=("scan256", "point1m", "events_csitl",
                                            "events_bgo_surrogate"),
                     default="scan256")
-    ap.add_argument("--events", type=int, default=10_000,
+    ap.add_argument("--events", type=int, default=50_000,
                     help="events in the secondary events/s measurement of the default run "
+                         "(runs/gammas_csitl_50k.toml: 50,000; 0 = skip)")
+    ap.add_argument("--point1m", type=int, default=1,
+                    help="add the 10^6-photon CsI(Tl)+Teflon point source to the default line "
                          "(0 = skip)")
+    ap.add_argument("--tune-events", type=int, default=5_000,
+                    help="events of the sample the launch-shape autotuner times")
     ap.add_argument("--surrogate-training", type=int, default=1,
                     help="add the surrogate MLP's training throughput to the default line (0 = skip)")
     ap.add_argument("--surrogate-events", type=int, default=500_000,

@@ -22,7 +22,7 @@ EXPORTS = (
     "cl_run_segments_device", "cl_sync", "cl_last_steps", "cl_set_launch",
     "cl_debug_eval", "cl_run_photons_noalloc", "cl_run_segments_moments_device",
     "cl_run_events_surrogate_device", "cl_surrogate_combine", "cl_debug_sampler",
-    "cl_surrogate_inputs",
+    "cl_surrogate_inputs", "cl_set_time_budget",
 )
 
 # Fixed-point scales of cl_run_segments_moments_device (crysplight_cuda.h)
@@ -36,6 +36,10 @@ CL_ERR_CUDA = -2
 CL_ERR_OOM = -3
 CL_ERR_TIMEOUT = -4
 CL_ERR_STATE = -5
+
+# include/crysplight_cuda.h: CL_MAX_BOUNCES_LIMIT, CL_DEFAULT_TIME_BUDGET_S
+MAX_BOUNCES_LIMIT = 10_000_000
+DEFAULT_TIME_BUDGET_S = 300.0
 
 
 class LibraryNotBuilt(RuntimeError):
@@ -92,6 +96,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.cl_last_steps.restype = C.c_int64
     lib.cl_set_launch.argtypes = [_P, C.c_int, C.c_int, C.c_int]
     lib.cl_set_launch.restype = C.c_int
+    lib.cl_set_time_budget.argtypes = [_P, C.c_double]
+    lib.cl_set_time_budget.restype = C.c_int
     lib.cl_debug_eval.argtypes = [_P, C.c_int, _P, _P, C.c_int64, C.c_uint64, C.c_int32]
     lib.cl_debug_eval.restype = C.c_int
     lib.cl_run_photons_noalloc.argtypes = common[1:] + [

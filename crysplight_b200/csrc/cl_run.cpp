@@ -389,6 +389,9 @@ GammaSetup load_gamma_setup(const std::string& cfg_arg, const std::string& data_
     const Table& camp = table(cfg, "campaign", g.cfg_path);
     g.tag = str(need(camp, "tag", "[campaign]"), "campaign.tag");
     g.n_events = integer(need(camp, "n_events", "[campaign]"), "campaign.n_events");
+    if (g.n_events < 1)
+        throw std::runtime_error(g.cfg_path + ": campaign.n_events must be >= 1 (got " +
+                                 std::to_string(g.n_events) + ")");
     g.seed = (uint64_t)integer(need(camp, "seed", "[campaign]"), "campaign.seed");
     const Table& crystal_cfg = table(cfg, "crystal", g.cfg_path);
     g.crystal_name = str(need(crystal_cfg, "material", "[crystal]"), "crystal.material");
@@ -585,14 +588,21 @@ int run_gamma(cl_handle* h, const GammaSetup& g, bool write)
     const double nn = (double)std::max<int64_t>(n, 1);
     std::printf("%-14s %lld events (%.1fs, cuda): interacted %.1f%%, photopeak %.1f%%\n", g.tag.c_str(),
                 (long long)n, elapsed, 100.0 * inter / nn, 100.0 * pe.size() / nn);
-    if (pe.size() > 1) {
+    if (!pe.empty()) {
+        // as the reference: printed for any photopeak event; one event has no
+        // sample standard deviation (Julia's std gives NaN)
         double mean = 0.0, var = 0.0;
         for (double v : pe) mean += v;
         mean /= pe.size();
         for (double v : pe) var += (v - mean) * (v - mean);
-        const double sd = std::sqrt(var / (pe.size() - 1));
-        std::printf("%-14s photopeak: %.0f pe mean, FWHM/mean %.2f%% (photostatistics+transport only)\n", "",
-                    mean, 235.5 * sd / mean);
+        if (pe.size() > 1) {
+            const double sd = std::sqrt(var / (pe.size() - 1));
+            std::printf("%-14s photopeak: %.0f pe mean, FWHM/mean %.2f%% (photostatistics+transport only)\n",
+                        "", mean, 235.5 * sd / mean);
+        } else {
+            std::printf("%-14s photopeak: %.0f pe mean, FWHM/mean NaN%% (photostatistics+transport only)\n",
+                        "", mean);
+        }
     }
     std::fflush(stdout);
     return 0;
@@ -658,7 +668,8 @@ int main(int argc, char** argv)
             j.gamma = cltoml::parse_file(absolute(f)).count("campaign") != 0;
             if (j.gamma) {
                 j.campaign = load_gamma_setup(f, data_dir, out_root);
-                if (ev_override >= 0) j.campaign.n_events = ev_override;
+                if (ev_override == 0) throw std::runtime_error("--n-events must be >= 1");
+                if (ev_override > 0) j.campaign.n_events = ev_override;
             } else {
                 j.point = load_setup(f, data_dir, out_root);
                 if (n_override >= 0) j.point.n_photons = n_override;

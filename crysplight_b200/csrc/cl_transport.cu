@@ -91,7 +91,16 @@ struct KArgs {
     unsigned int* done;
     unsigned int* err;
     const float* logtab;  // log of every uniform (k+1)*2^-24 at [k], or NULL: compute
+    unsigned long long budget_ns;   // device time budget of the launch, 0 = none
 };
+
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ int time_bin0(float t, const Physics& P)
 {
@@ -216,7 +225,10 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
     // warp-uniform work pool
     int64_t pool_lo = 0, pool_hi = 0, pool_src = 0;
     bool exhausted = false;
-    bool overrun = false, under = false;
+    bool overrun = false, under = false, timed_out = false;
+    // time budget: a warp-uniform iteration count, the clock read every 256
+    uint32_t iter = 0;
+    const unsigned long long t_begin = A.budget_ns ? globaltimer_ns() : 0ull;
 
     for (;;) {
         // ---- refill idle lanes from the warp's pool / the global queue ----
@@ -273,6 +285,10 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
             }
         }
         if (!__any_sync(FULL, st != S_IDLE)) break;
+        if (A.budget_ns != 0ull && ((++iter) & 255u) == 0u) {
+            // photons still in flight are dropped; the host reports CL_ERR_TIMEOUT
+            if (__any_sync(FULL, globaltimer_ns() - t_begin > A.budget_ns)) { timed_out = true; break; }
+        }
 
         // ---- top up the uniform ring: one Philox call site for the warp ----
         {
@@ -600,6 +616,7 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
     }
     if (overrun) atomicOr(A.err, 1u);
     if (under) atomicOr(A.err, 2u);
+    if (timed_out && lane == 0) atomicOr(A.err, 32u);
     __syncthreads();
 
     // ---- one coalesced flush per CTA ----
@@ -756,6 +773,7 @@ struct cl_handle {
     int warp_chunk = CL_DEFAULT_WARP_CHUNK;   // 0: automatic per launch
     int64_t last_steps = 0;
     int max_smem_optin = 0;
+    unsigned long long budget_ns = (unsigned long long)(CL_DEFAULT_TIME_BUDGET_S * 1e9);
 };
 
 static thread_local char g_create_err[512];
@@ -913,13 +931,26 @@ int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta, int warp_c
     return CL_OK;
 }
 
+int cl_set_time_budget(cl_handle* h, double seconds)
+{
+    if (!h) return CL_ERR_STATE;
+    if (!(seconds >= 0.0) || !std::isfinite(seconds) || seconds > 1.0e9)
+        return set_err(h, CL_ERR_ARG, "time budget must be finite, >= 0 and <= 1e9 s");
+    h->budget_ns = (unsigned long long)(seconds * 1e9);
+    return CL_OK;
+}
+
 }  // extern "C"
 
 // ---- argument validation shared by the entry points ----
 static int check_params(cl_handle* h, const cl_box* box, const cl_optical_params* op,
-                        const cl_readout* ro, const cl_time_binning* tb, float tau_ns)
+                        const cl_readout* ro, const cl_time_binning* tb, float tau_ns,
+                        int32_t max_bounces)
 {
     if (!box || !op || !ro || !tb) return set_err(h, CL_ERR_ARG, "null parameter struct");
+    if (max_bounces > CL_MAX_BOUNCES_LIMIT)
+        return set_err(h, CL_ERR_ARG, "max_bounces %d above the limit %d", (int)max_bounces,
+                       (int)CL_MAX_BOUNCES_LIMIT);
     for (int i = 0; i < 3; ++i)
         if (!(box->L[i] > 0.0f) || !std::isfinite(box->L[i]))
             return set_err(h, CL_ERR_ARG, "box sizes must be finite and positive");
@@ -1046,6 +1077,7 @@ static int enqueue_point(cl_handle* h, const Physics& P, const float* px, const 
     if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
     a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
     a.logtab = (const float*)h->logtab.p;
+    a.budget_ns = h->budget_ns;
     const size_t tile_bytes = ((size_t)n_counts + cells) * sizeof(uint32_t);
     const size_t base_bytes = LOGTAB_BYTES + (size_t)RING_LEN * RING_STRIDE * sizeof(float);
     const bool tile = base_bytes + tile_bytes <= (size_t)std::min(h->max_smem_optin, 160 * 1024);
@@ -1087,6 +1119,7 @@ static int enqueue_segments(cl_handle* h, const Physics& P, const float* sx, con
         if (want_rec) { a.r_status = rec->status; a.r_idx = rec->idx; a.r_t = rec->t; a.r_bounces = rec->bounces; }
         a.queue = s.queue; a.steps = s.steps; a.done = s.done; a.err = s.err;
         a.logtab = (const float*)h->logtab.p;
+        a.budget_ns = h->budget_ns;
         const size_t smem = LOGTAB_BYTES + (size_t)RING_LEN * RING_STRIDE * sizeof(float);
         a.tsum = tsum; a.tsum2 = tsum2;
         const int rc = moments ? launch_transport<2, false, false>(h, a, smem, st)
@@ -1114,6 +1147,9 @@ static int collect(cl_handle* h, cudaStream_t st)
     CK(h, cudaMemcpyAsync(&err, s.err, sizeof err, cudaMemcpyDeviceToHost, st), "copy status");
     CK(h, cudaStreamSynchronize(st), "stream synchronize");
     h->last_steps = (int64_t)steps;
+    if (err & 32u)
+        return set_err(h, CL_ERR_TIMEOUT, "the transport ran past the handle's time budget (%.3g s); "
+                       "its outputs are incomplete", (double)h->budget_ns * 1e-9);
     if (err & 2u) return set_err(h, CL_ERR_CUDA, "internal error: uniform ring underflow in the transport kernel");
     if (err & 16u) return set_err(h, CL_ERR_ARG, "a source's segment id is out of range (its detections were dropped)");
     if (err & 8u) return set_err(h, CL_ERR_ARG, "a surrogate site's segment id is out of range (site skipped)");
@@ -1135,7 +1171,7 @@ int cl_run_photons(cl_handle* h, const cl_box* box, const cl_optical_params* op,
 {
     if (!h) return CL_ERR_STATE;
     h->err[0] = 0;
-    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    int rc = check_params(h, box, op, ro, tb, tau_ns, max_bounces);
     if (rc != CL_OK) return rc;
     if (npos < 1 || !px || !py || !pz) return set_err(h, CL_ERR_ARG, "need npos >= 1 source positions");
     if (n_photons < 0) return set_err(h, CL_ERR_ARG, "n_photons must be >= 0");
@@ -1208,7 +1244,7 @@ int cl_run_photons_device(cl_handle* h, const cl_box* box, const cl_optical_para
 {
     if (!h) return CL_ERR_STATE;
     h->err[0] = 0;
-    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    int rc = check_params(h, box, op, ro, tb, tau_ns, max_bounces);
     if (rc != CL_OK) return rc;
     if (npos < 1 || !d_px || !d_py || !d_pz) return set_err(h, CL_ERR_ARG, "need npos >= 1 source positions");
     if (n_photons < 0) return set_err(h, CL_ERR_ARG, "n_photons must be >= 0");
@@ -1247,7 +1283,7 @@ int cl_run_segments(cl_handle* h, const cl_box* box, const cl_optical_params* op
 {
     if (!h) return CL_ERR_STATE;
     h->err[0] = 0;
-    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    int rc = check_params(h, box, op, ro, tb, tau_ns, max_bounces);
     if (rc != CL_OK) return rc;
     int64_t n = 0;
     if ((rc = check_segments(h, src_offsets, src_segment, n_src, n_segments, &n)) != CL_OK) return rc;
@@ -1329,7 +1365,7 @@ int cl_run_segments_device(cl_handle* h, const cl_box* box, const cl_optical_par
 {
     if (!h) return CL_ERR_STATE;
     h->err[0] = 0;
-    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    int rc = check_params(h, box, op, ro, tb, tau_ns, max_bounces);
     if (rc != CL_OK) return rc;
     if (n_src < 1 || n_segments < 1) return set_err(h, CL_ERR_ARG, "need n_src >= 1 and n_segments >= 1");
     if (!d_sx || !d_sy || !d_sz || !d_src_offsets || !d_src_segment)
@@ -1358,7 +1394,7 @@ int cl_run_segments_moments_device(cl_handle* h, const cl_box* box, const cl_opt
 {
     if (!h) return CL_ERR_STATE;
     h->err[0] = 0;
-    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    int rc = check_params(h, box, op, ro, tb, tau_ns, max_bounces);
     if (rc != CL_OK) return rc;
     if (n_src < 1 || n_segments < 1) return set_err(h, CL_ERR_ARG, "need n_src >= 1 and n_segments >= 1");
     if (!d_sx || !d_sy || !d_sz || !d_src_offsets || !d_src_segment)
@@ -1390,7 +1426,7 @@ int cl_run_events_surrogate_device(cl_handle* h, const cl_box* box, const cl_opt
 {
     if (!h) return CL_ERR_STATE;
     h->err[0] = 0;
-    int rc = check_params(h, box, op, ro, tb, tau_ns);
+    int rc = check_params(h, box, op, ro, tb, tau_ns, max_bounces);
     if (rc != CL_OK) return rc;
     if (n_segments < 1) return set_err(h, CL_ERR_ARG, "need n_segments >= 1");
     if (n_src < 0 || n_sites < 0 || n_photons < 0) return set_err(h, CL_ERR_ARG, "negative size");
@@ -1538,7 +1574,7 @@ extern "C" int cl_run_photons_noalloc(const cl_box* box, const cl_optical_params
         snprintf(g_create_err, sizeof g_create_err, "cl_run_photons_noalloc: %s", tmp.err);
         return rc;
     };
-    int rc = check_params(&tmp, box, op, ro, tb, tau_ns);
+    int rc = check_params(&tmp, box, op, ro, tb, tau_ns, max_bounces);
     if (rc != CL_OK) return fail(rc);
     if (npos < 1 || !px || !py || !pz) return fail(set_err(&tmp, CL_ERR_ARG, "need npos >= 1 source positions"));
     if (n_photons < 0) return fail(set_err(&tmp, CL_ERR_ARG, "n_photons must be >= 0"));

@@ -284,7 +284,10 @@ def sample_sites(engine, box: Box, op: OpticalParams, ro: Readout, tb: TimeBinni
         stream_arg(stream))
     eng._check(rc)
     eng.sync(stream)
+    wall = torch.from_numpy((flag_h & 2) != 0).to(dev)
     stats = {"sites": n_sites, "fallback_sites": int(fb.size), "photons_mc": n_mc,
+             "photons_total": int(photons.sum().item()),
+             "photons_wall": int(photons[wall].sum().item()) if bool(wall.any()) else 0,
              "flag_spread": int(np.count_nonzero(flag_h & 1)),
              "flag_wall": int(np.count_nonzero(flag_h & 2)),
              "flag_invalid": int(np.count_nonzero(flag_h & 4))}

@@ -62,6 +62,42 @@ def segment_range(photons_per_segment: Sequence[int], rank: int, world: int) -> 
     return lo, hi, int(c[lo])
 
 
+def check_segments(photons_per_source, segment_of_source, n_segments: int):
+    """Validate a segmented job as cl_run_segments does (src/events.jl:70,88
+    numbers photons event-major, so the photons before a range of whole
+    segments are the photons of the sources before it only when segment ids
+    never decrease along the sources): returns (counts int64, segment int64)
+    or raises ValueError.  Every rank checks the same arrays, so all ranks
+    raise before any collective."""
+    cnt = np.asarray(photons_per_source, np.int64).reshape(-1)
+    seg = np.asarray(segment_of_source, np.int64).reshape(-1)
+    if cnt.shape != seg.shape:
+        raise ValueError("photons_per_source and segment_of_source differ in length")
+    if int(n_segments) < 1:
+        raise ValueError("need n_segments >= 1")
+    if cnt.size and (cnt.min() < 0):
+        raise ValueError("photons_per_source must be >= 0")
+    if seg.size and (seg.min() < 0 or seg.max() >= int(n_segments)):
+        raise ValueError("segment id out of range")
+    if seg.size > 1 and np.any(np.diff(seg) < 0):
+        raise ValueError("segment ids must be non-decreasing along the sources "
+                         "(photon ids are numbered segment-major)")
+    return cnt, seg
+
+
+def shard_segments(photons_per_source, segment_of_source, n_segments: int, rank: int, world: int):
+    """Rank ``rank``'s share of a segmented job: (first segment, end segment,
+    first source, end source, photons before the first source).  The sources
+    of segments [lo, hi) are the contiguous range [s0, s1) because segment ids
+    are non-decreasing (checked)."""
+    cnt, seg = check_segments(photons_per_source, segment_of_source, n_segments)
+    per_seg = np.bincount(seg, weights=cnt, minlength=int(n_segments)).astype(np.int64)
+    lo, hi, _ = segment_range(per_seg, rank, world)
+    s0 = int(np.searchsorted(seg, lo, side="left"))
+    s1 = int(np.searchsorted(seg, hi, side="left"))
+    return lo, hi, s0, s1, int(cnt[:s0].sum())
+
+
 def reduce_accumulator(acc: Accumulator, group=None) -> Accumulator:
     """All-reduce a per-rank Accumulator in place: counts and counters summed,
     first-hit times by min (src/transport.jl:82-91, ``merge!``)."""
@@ -145,19 +181,18 @@ def run_segments_sharded(runner: Callable, *, sources, photons_per_source, segme
     import torch.distributed as dist
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     src = np.asarray(sources, np.float32).reshape(-1, 3)
-    cnt = np.asarray(photons_per_source, np.int64).reshape(-1)
-    seg = np.asarray(segment_of_source, np.int64).reshape(-1)
-    per_seg = np.bincount(seg, weights=cnt, minlength=int(n_segments)).astype(np.int64)
-    lo, hi, before = segment_range(per_seg, rank, world)
-    sel = (seg >= lo) & (seg < hi)
+    cnt, seg = check_segments(photons_per_source, segment_of_source, n_segments)
+    if src.shape[0] != cnt.size:
+        raise ValueError("sources and photons_per_source differ in length")
+    lo, hi, s0, s1, before = shard_segments(cnt, seg, n_segments, rank, world)
     n_local = hi - lo
-    first_src = int(np.argmax(sel)) if sel.any() else 0
-    pid0 = pid_offset + int(cnt[:first_src].sum()) if sel.any() else pid_offset + before
+    pid0 = pid_offset + before
     res = None
     cells_shape = kw.pop("cells_shape", (8, 8))
-    if n_local > 0 and sel.any():
-        res = runner(sources=src[sel], photons_per_source=cnt[sel], segment_of_source=(seg[sel] - lo),
-                     n_segments=n_local, t0s=None if t0s is None else np.asarray(t0s, np.float32)[sel],
+    if n_local > 0 and s1 > s0:
+        res = runner(sources=src[s0:s1], photons_per_source=cnt[s0:s1],
+                     segment_of_source=(seg[s0:s1] - lo), n_segments=n_local,
+                     t0s=None if t0s is None else np.asarray(t0s, np.float32)[s0:s1],
                      pid_offset=pid0, **kw)
         get = (lambda k: res[k]) if isinstance(res, dict) else (lambda k: getattr(res, k))
         maps, tmin, npe, ctr = get("maps"), get("tmin"), get("npe"), get("counters")
@@ -172,3 +207,89 @@ def run_segments_sharded(runner: Callable, *, sources, photons_per_source, segme
     c = torch.tensor([int(ctr[n]) if ctr else 0 for n in COUNTER_NAMES], dtype=torch.int64, device=dev)
     dist.all_reduce(c, op=dist.ReduceOp.SUM, group=group)
     return maps_all, tmin_all, npe_all, dict(zip(COUNTER_NAMES, (int(v) for v in c.cpu().tolist())))
+
+
+class ShardedSegments:
+    """A segmented job split over the ranks of ``group`` with the inputs of
+    this rank's share resident on its GPU: ``step()`` enqueues the transport
+    of the share (one ``cl_run_segments_device`` launch sequence, as
+    ``batching.DeviceEvents``) and then gathers every rank's per-segment maps,
+    first-hit times and npe into device tensors on every rank (NCCL
+    all_gather, shares padded to the largest) and sums the counters
+    (all_reduce).  The host arrays describing the job are the same on every
+    rank; photon ids are numbered over the whole job, so the gathered maps
+    equal one single-GPU call bit for bit."""
+
+    def __init__(self, engine, box, op, ro, tb, *, sources, photons_per_source, segment_of_source,
+                 n_segments: int, seed: int, tau_ns: float, t0s=None, pid_offset: int = 0,
+                 max_bounces: int = 100_000, group=None):
+        import torch
+        import torch.distributed as dist
+        from .batching import DeviceEvents
+        self.group = group
+        self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
+        src = np.asarray(sources, np.float32).reshape(-1, 3)
+        cnt, seg = check_segments(photons_per_source, segment_of_source, n_segments)
+        if src.shape[0] != cnt.size:
+            raise ValueError("sources and photons_per_source differ in length")
+        self.n_segments = int(n_segments)
+        self.plans = [shard_segments(cnt, seg, n_segments, r, self.world) for r in range(self.world)]
+        lo, hi, s0, s1, before = self.plans[self.rank]
+        self.n_local = hi - lo
+        self.n_max = max(p[1] - p[0] for p in self.plans)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        t0 = np.zeros(src.shape[0], np.float32) if t0s is None else np.asarray(t0s, np.float32)
+        self.local = None
+        if self.n_local > 0 and s1 > s0:
+            self.local = DeviceEvents(engine, box, op, ro, tb, xyz=T(src[s0:s1]), t0=T(t0[s0:s1]),
+                                      photons=T(cnt[s0:s1]), segment=T((seg[s0:s1] - lo).astype(np.int32)),
+                                      n_segments=self.n_local, seed=seed, tau_ns=tau_ns,
+                                      pid_offset=pid_offset + before, max_bounces=max_bounces)
+        self.cells = (ro.grid if hasattr(ro, "grid") else ro).nx * (ro.grid if hasattr(ro, "grid") else ro).ny
+        self.n_photons_local = int(cnt[s0:s1].sum())
+        # padded send buffers and gathered outputs
+        self.send_maps = torch.zeros(self.cells * self.n_max, dtype=torch.int32, device=dev)
+        self.send_tmin = torch.full((self.cells * self.n_max,), float("inf"), dtype=torch.float32, device=dev)
+        self.send_npe = torch.zeros(self.n_max, dtype=torch.int32, device=dev)
+        self.maps_all = torch.empty(self.world * self.cells * self.n_max, dtype=torch.int32, device=dev)
+        self.tmin_all = torch.empty(self.world * self.cells * self.n_max, dtype=torch.float32, device=dev)
+        self.npe_all = torch.empty(self.world * self.n_max, dtype=torch.int32, device=dev)
+        self.counters = torch.zeros(9, dtype=torch.int64, device=dev)
+
+    def step(self, stream=None) -> None:
+        """Transport this rank's share, then gather all shares (device work
+        only; every rank takes the same collective steps)."""
+        import torch
+        import torch.distributed as dist
+        n = self.cells * self.n_local
+        if self.local is not None:
+            self.local.step(stream)
+            self.send_maps[:n].copy_(self.local.maps)
+            self.send_tmin[:n].copy_(self.local.tmin)
+            self.send_npe[:self.n_local].copy_(self.local.npe)
+            self.counters.copy_(self.local.counters)
+        else:
+            self.counters.zero_()
+        dist.all_gather_into_tensor(self.maps_all, self.send_maps, group=self.group)
+        dist.all_gather_into_tensor(self.tmin_all, self.send_tmin, group=self.group)
+        dist.all_gather_into_tensor(self.npe_all, self.send_npe, group=self.group)
+        dist.all_reduce(self.counters, op=dist.ReduceOp.SUM, group=self.group)
+
+    def sync(self) -> None:
+        """Wait for the device and report this rank's transport errors."""
+        if self.local is not None:
+            self.local.sync()
+
+    def result(self):
+        """(maps (nx*ny, n_segments) uint32, tmin, npe, counters dict) on the host,
+        the padding of the shares removed."""
+        from .params import COUNTER_NAMES
+        maps = self.maps_all.cpu().numpy().view(np.uint32).reshape(self.world, self.n_max, self.cells)
+        tmin = self.tmin_all.cpu().numpy().reshape(self.world, self.n_max, self.cells)
+        npe = self.npe_all.cpu().numpy().reshape(self.world, self.n_max)
+        k = [p[1] - p[0] for p in self.plans]
+        maps = np.concatenate([maps[r, :k[r]] for r in range(self.world)], axis=0).T
+        tmin = np.concatenate([tmin[r, :k[r]] for r in range(self.world)], axis=0).T
+        npe = np.concatenate([npe[r, :k[r]] for r in range(self.world)])
+        return maps, tmin, npe, dict(zip(COUNTER_NAMES, self.counters.cpu().tolist()))

@@ -56,6 +56,8 @@ def load_gamma_setup(cfg_path: str, data_dir: Optional[str] = None) -> GammaSetu
         cfg = tomllib.load(f)
     data_dir = data_dir or _data_dir_for(cfg_path)
     camp = cfg["campaign"]
+    if int(camp["n_events"]) < 1:
+        raise ValueError(f"{cfg_path}: campaign.n_events must be >= 1 (got {camp['n_events']})")
     mat = load_material(cfg["crystal"]["material"], data_dir)
     wrap = load_material(cfg["wrap"]["material"], data_dir)
     sipm = load_material(cfg["sipm"]["material"], data_dir)
@@ -98,10 +100,14 @@ def summary(st: GammaSetup, r, elapsed: float, backend: str) -> dict:
     print(f"{st.tag:<14s} {n} events ({elapsed:.1f}s, {backend}): interacted "
           f"{100 * interacted.mean():.1f}%, photopeak {100 * peak.mean():.1f}%")
     pe = r.npe[peak].astype(np.float64)
-    if pe.size > 1:
-        m, s = pe.mean(), pe.std(ddof=1)
+    if pe.size > 0:
+        # printed for any photopeak event, as the reference; one event has no
+        # sample standard deviation (NaN, as Julia's std)
+        m = pe.mean()
+        s = pe.std(ddof=1) if pe.size > 1 else float("nan")
         out.update({"photopeak_pe_mean": float(m), "photopeak_fwhm_rel": float(2.355 * s / m)})
-        print(f"{'':<14s} photopeak: {m:.0f} pe mean, FWHM/mean {235.5 * s / m:.2f}% "
+        fw = f"{235.5 * s / m:.2f}" if pe.size > 1 else "NaN"
+        print(f"{'':<14s} photopeak: {m:.0f} pe mean, FWHM/mean {fw}% "
               "(photostatistics+transport only)")
     return out
 
@@ -114,6 +120,8 @@ def shoot_gammas(cfg_path: str, *, engine=None, surrogate=None, write: bool = Tr
     from .transport import default_engine
     st = load_gamma_setup(cfg_path, data_dir)
     if n_events is not None:
+        if int(n_events) < 1:
+            raise ValueError("n_events must be >= 1")
         st.n_events = int(n_events)
     mat = GammaMaterial.from_csv(st.crystal_name, st.density, st.xcom_path)
     eng = engine or default_engine()

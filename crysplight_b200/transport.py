@@ -106,6 +106,11 @@ class Engine:
     def set_launch(self, ctas_per_sm: int = 0, threads_per_cta: int = 0, warp_chunk: int = 0) -> None:
         self._check(self.lib.cl_set_launch(self.handle, ctas_per_sm, threads_per_cta, warp_chunk))
 
+    def set_time_budget(self, seconds: float) -> None:
+        """Device time budget of every transport launch on this engine (0 = none):
+        a launch that runs longer stops and the call raises CL_ERR_TIMEOUT."""
+        self._check(self.lib.cl_set_time_budget(self.handle, float(seconds)))
+
     # -- run_photons_ka!, src/kernel.jl:312-367 --------------------------------
     def run_photons_ka(self, box: Box, op: OpticalParams, ro, tb: TimeBinning, *,
                        n_photons: int, seed: int, pos=None, positions=None, t0s=None,

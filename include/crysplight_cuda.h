@@ -60,6 +60,16 @@ extern "C" {
 #define CL_ERR_TIMEOUT  -4   /* a device-side loop budget ran out                       */
 #define CL_ERR_STATE    -5   /* handle misuse (null handle, wrong device)               */
 
+/* Largest max_bounces the transport entry points accept (CL_ERR_ARG above).
+ * The reference's default is 100,000 (src/config.jl:68, src/kernel.jl:318);
+ * values <= 0 are accepted and, as in the reference (src/transport.jl:140,229),
+ * cap every photon at its first wall interaction or scatter. */
+#define CL_MAX_BOUNCES_LIMIT 10000000
+
+/* Device time budget of a transport launch on a new handle, in seconds
+ * (cl_set_time_budget). */
+#define CL_DEFAULT_TIME_BUDGET_S 300.0
+
 /* Box, src/geometry.jl:14-16: crystal [0,L0]x[0,L1]x[0,L2] in mm. */
 typedef struct cl_box {
     float L[3];
@@ -354,6 +364,19 @@ int64_t cl_last_steps(const cl_handle* h);
  */
 int cl_set_launch(cl_handle* h, int ctas_per_sm, int threads_per_cta,
                   int warp_chunk);
+
+/*
+ * Device-side time budget of every transport launch on this handle: the
+ * kernel's warps stop once the launch has run `seconds` of wall-clock time on
+ * the GPU, and the call (or cl_sync for the *_device calls) returns
+ * CL_ERR_TIMEOUT; the outputs of such a call are incomplete.  It bounds the
+ * time a launch can hold a shared GPU whatever n_photons x max_bounces is
+ * (photons trapped by total internal reflection in an ideal reflector bounce
+ * until max_bounces).  0 = no budget; default CL_DEFAULT_TIME_BUDGET_S.  The
+ * reference has no counterpart (its loop is bounded by max_bounces alone,
+ * src/transport.jl:228-232).  CL_ERR_ARG for a negative or non-finite value.
+ */
+int cl_set_time_budget(cl_handle* h, double seconds);
 
 /*
  * Diagnostics for tests: evaluate the device's Float32 elementary functions

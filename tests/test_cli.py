@@ -243,3 +243,34 @@ def test_cli_run_writes_the_same_light_h5_as_python(cli, tmp_path):
         assert r.returncode == 0, r.stderr
         assert "detected" in r.stdout
         assert (tmp_path / f"{tag}.py.h5").read_bytes() == py_file.read_bytes()
+
+
+def test_campaign_without_events_is_an_error(cli, tmp_path):
+    """campaign.n_events < 1 (in the run file or from --n-events) is rejected
+    with a message, by the C++ program and by the Python loader."""
+    runs = tmp_path / "runs"
+    runs.mkdir()
+    txt = open(GAMMA_RUNS[0]).read()
+    import re
+    p = runs / "zero.toml"
+    p.write_text(re.sub(r"n_events\s*=\s*[0-9_]+", "n_events = 0", txt))
+    r = subprocess.run([cli, "--print-setup", "--data", os.path.join(PKG, "data"), str(p)],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "n_events must be >= 1" in r.stderr
+    with pytest.raises(ValueError):
+        load_gamma_setup(str(p), data_dir=os.path.join(PKG, "data"))
+    r = subprocess.run([cli, "--print-setup", "--n-events", "0", GAMMA_RUNS[0]], capture_output=True, text=True)
+    assert r.returncode != 0 and "n-events" in r.stderr
+
+
+def test_summary_with_one_photopeak_event(capsys):
+    """The reference prints the photopeak line whenever a photopeak event
+    exists (scripts/shoot_gammas.jl:86-89); with one event the width is NaN."""
+    from types import SimpleNamespace
+    from crysplight_b200.shoot_gammas import summary
+    st = load_gamma_setup(GAMMA_RUNS[0])
+    st.n_events = 3
+    r = SimpleNamespace(edep=np.float32([511.0, 0.0, 300.0]), npe=np.int32([9800, 0, 5000]))
+    out = summary(st, r, 1.0, "cuda")
+    line = capsys.readouterr().out.splitlines()[-1]
+    assert "9800 pe mean" in line and "NaN%" in line and out["photopeak_pe_mean"] == 9800.0

@@ -124,3 +124,68 @@ def test_transport_source_with_a_bad_segment_is_reported(engine):
         engine.sync(st.cuda_stream)
     assert e.value.code == _lib.CL_ERR_ARG
     assert int(maps[64:].sum()) == 0 and int(npe[0]) == int(maps[:64].sum()) > 0
+
+
+def test_max_bounces_above_the_limit_is_rejected(engine):
+    """max_bounces above CL_MAX_BOUNCES_LIMIT is an argument error at every
+    transport entry point (nothing is launched); <= 0 caps every photon at its
+    first interaction, as src/transport.jl:228-232 does."""
+    from crysplight_b200 import _lib
+    from crysplight_b200._lib import CudaTransportError
+    from crysplight_b200.params import Counters, Readout
+    big = _lib.MAX_BOUNCES_LIMIT + 1
+    with pytest.raises(CudaTransportError) as e:
+        engine.run_photons_ka(BOX_BGO, OP_BGO_ESR, GRID, TB80, n_photons=100, seed=1,
+                              pos=(24.0, 24.0, 11.2), tau_ns=0.0, max_bounces=big)
+    assert e.value.code == _lib.CL_ERR_ARG and b"max_bounces" in engine.lib.cl_last_error(engine.handle)
+    with pytest.raises(CudaTransportError) as e:
+        engine.run_segments(BOX_BGO, OP_BGO_ESR, GRID, TB80, sources=[(24.0, 24.0, 11.2)],
+                            photons_per_source=[100], segment_of_source=[0], n_segments=1, seed=1,
+                            tau_ns=0.0, max_bounces=big)
+    assert e.value.code == _lib.CL_ERR_ARG
+    lib = _lib.load()
+    p = np.float32([24.0])
+    z = np.float32([11.2])
+    counts = np.zeros(64 * 81, np.uint32)
+    first = np.zeros(64, np.float32)
+    ctr = Counters()
+    f = lambda a: a.ctypes.data_as(C.c_void_p)
+    rc = lib.cl_run_photons_noalloc(C.byref(BOX_BGO), C.byref(OP_BGO_ESR), C.byref(Readout(GRID)),
+                                    C.byref(TB80), f(p), f(p), f(z), None, 1, 100, 1, 0, 0.0, big,
+                                    f(counts), f(first), C.byref(ctr), None)
+    assert rc == _lib.CL_ERR_ARG and b"max_bounces" in lib.cl_last_error(None)
+    # at the limit and at 0 the calls run; 0 caps each photon at its first bounce
+    acc = engine.run_photons_ka(BOX_BGO, OP_BGO_ESR, GRID, TB80, n_photons=1000, seed=1,
+                                pos=(24.0, 24.0, 11.2), tau_ns=0.0, max_bounces=0)
+    assert acc.total_terminated() == 1000 and acc.ncap > 0
+
+
+def test_time_budget_stops_a_launch_of_trapped_photons(engine):
+    """Photons trapped by total internal reflection in an ideal specular box
+    (src/transport.jl:228-232 bounds them by max_bounces only) keep a launch
+    busy; the device time budget ends it with CL_ERR_TIMEOUT in about the
+    budget's time and the handle stays usable.  Bounded without the budget
+    too: 2048 photons (one per lane) x 2,000,000 bounces."""
+    import time
+    from crysplight_b200 import _lib
+    from crysplight_b200._lib import CudaTransportError
+    from cases import BOX_CSI, CENTRE_CSI, ideal
+    trap = ideal(1.95, spec=True)              # wrap R = 1, no absorption, polished
+    assert engine.lib.cl_set_time_budget(engine.handle, -1.0) == _lib.CL_ERR_ARG
+    assert engine.lib.cl_set_time_budget(engine.handle, float("nan")) == _lib.CL_ERR_ARG
+    engine.set_time_budget(0.02)
+    try:
+        t0 = time.perf_counter()
+        with pytest.raises(CudaTransportError) as e:
+            engine.run_photons_ka(BOX_CSI, trap, GRID, TB80, n_photons=2048, seed=5, pos=CENTRE_CSI,
+                                  tau_ns=0.0, max_bounces=2_000_000)
+        dt = time.perf_counter() - t0
+        assert e.value.code == _lib.CL_ERR_TIMEOUT
+        assert b"time budget" in engine.lib.cl_last_error(engine.handle)
+        assert dt < 2.0, dt
+    finally:
+        engine.set_time_budget(_lib.DEFAULT_TIME_BUDGET_S)
+    # the same photons with the reference's default cap run to completion
+    acc = engine.run_photons_ka(BOX_CSI, trap, GRID, TB80, n_photons=2048, seed=5, pos=CENTRE_CSI,
+                                tau_ns=0.0, max_bounces=20_000)
+    assert acc.total_terminated() == 2048 and acc.ncap > 0

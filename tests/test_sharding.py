@@ -94,3 +94,62 @@ def test_sharded_events_equal_single_run(sharded, oracle):
         assert np.array_equal(r["npe"], ref["npe"])
         assert r["ectr"].tolist() == list(ref["counters"].values())
         assert ref["npe"].sum() > 0 and (ref["npe"] == 0).any()     # segments with and without light
+
+
+def _reject_worker(rank, world, port, outdir):
+    import torch.distributed as dist
+    from crysplight_b200 import sharding
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    msgs = []
+    try:
+        calls = []
+        runner = lambda **kw: calls.append(kw)
+        pts = np.zeros((4, 3), np.float32)
+        for seg, n_seg in (([0, 2, 1, 3], 4), ([0, 1, 1, 5], 4), ([0, -1, 1, 2], 4)):
+            try:
+                sharding.run_segments_sharded(runner, sources=pts, photons_per_source=[10, 20, 30, 40],
+                                              segment_of_source=seg, n_segments=n_seg)
+                msgs.append("accepted")
+            except ValueError as e:
+                msgs.append(str(e))
+        # a valid job still goes through afterwards (same collective steps on every rank)
+        dist.barrier()
+        msgs.append(f"runner calls {len(calls)}")
+    finally:
+        dist.destroy_process_group()
+    with open(os.path.join(outdir, f"rank{rank}.txt"), "w") as f:
+        f.write("\n".join(msgs))
+
+
+def test_sharded_segments_reject_decreasing_segment_ids(tmp_path):
+    """Photon ids are numbered segment-major (src/events.jl:70,88): with a
+    segment id that decreases along the sources the photons before a rank's
+    range are not the photons of the sources before it, so every rank rejects
+    the job before any transport or collective."""
+    import torch.multiprocessing as mp
+    mp.spawn(_reject_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    for r in range(2):
+        lines = open(tmp_path / f"rank{r}.txt").read().splitlines()
+        assert "non-decreasing" in lines[0]
+        assert "out of range" in lines[1] and "out of range" in lines[2]
+        assert lines[3] == "runner calls 0"
+
+
+def test_shard_plans_cover_the_sources_once():
+    from crysplight_b200.sharding import check_segments, shard_segments
+    pts, cnt, seg, n_seg, t0 = _events()
+    for world in (1, 2, 3, 5, 8):
+        plans = [shard_segments(cnt, seg, n_seg, r, world) for r in range(world)]
+        assert plans[0][0] == 0 and plans[-1][1] == n_seg
+        assert plans[0][2] == 0 and plans[-1][3] == len(cnt)
+        for a, b in zip(plans, plans[1:]):
+            assert a[1] == b[0] and a[3] == b[2]
+        for lo, hi, s0, s1, before in plans:
+            assert before == int(cnt[:s0].sum())
+            assert all(lo <= s < hi for s in seg[s0:s1])
+    with pytest.raises(ValueError):
+        check_segments([1, 2], [1, 0], 2)
+    with pytest.raises(ValueError):
+        check_segments([1, -2], [0, 1], 2)
