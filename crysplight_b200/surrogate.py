@@ -268,6 +268,51 @@ def light_targets(scan: ScanResult) -> np.ndarray:
     return np.concatenate([logp, m1, logs], axis=1).astype(np.float32)
 
 
+def members_of_rank(members: int, rank: int, world: int) -> list:
+    """Ensemble members trained by ``rank`` of ``world`` (one GPU each):
+    rank, rank + world, ..."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("need 0 <= rank < world")
+    return list(range(rank, int(members), world))
+
+
+def _gather_members(trained: dict, members: int, world: int, group):
+    """All ranks receive every member's parameters and loss history, in member
+    order (all_gather of a (members per rank, P) block, padded)."""
+    import torch
+    import torch.distributed as dist
+    per = -(-members // world)
+    some = next(iter(trained.values()))[0] if trained else None
+    n_par = np.zeros(1, np.int64)
+    if some is not None:
+        n_par[0] = np.asarray(some).size
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+    t = torch.from_numpy(n_par).to(dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    P = int(t.item())
+    n_hist = max((len(h) for _, h in trained.values()), default=0)
+    t = torch.tensor([n_hist], dtype=torch.int64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    H = int(t.item())
+    block = np.zeros((per, P + H), np.float32)
+    rank = dist.get_rank(group)
+    for i, k in enumerate(members_of_rank(members, rank, world)):
+        p, h = trained[k]
+        block[i, :P] = np.asarray(p, np.float32)
+        block[i, P:P + len(h)] = np.asarray(h, np.float32)
+    src = torch.from_numpy(block).to(dev)
+    out = [torch.empty_like(src) for _ in range(world)]
+    dist.all_gather(out, src, group=group)
+    blocks = [o.cpu().numpy() for o in out]
+    params, history = [], []
+    for k in range(members):
+        r, i = k % world, k // world
+        params.append(blocks[r][i, :P].copy())
+        history.append([float(v) for v in blocks[r][i, P:P + H]])
+    return params, history
+
+
 def split_holdout(n_points: int, frac: float = 0.1, seed: int = 11):
     """Deterministic train / held-out split of point indices."""
     rng = np.random.default_rng(seed)
@@ -311,47 +356,74 @@ class LightSurrogate:
     def train(cls, box: Box, xyz: np.ndarray, targets: np.ndarray, *, members: int = 5, steps: int = 20000,
               batch: int = 65536, lr: float = 1e-3, lr_final: Optional[float] = None,
               time_weight: float = 1.0, z_warp: float = 0.0, z_range=None, seed: int = 0,
-              device: int = 0, chunk: int = 250, log=None):
+              device: int = 0, chunk: int = 250, log=None, group=None, member_trainer=None):
         """Train ``members`` networks on standardised targets.
 
         ``lr_final``: cosine decay of the Adam step size from ``lr`` to
         ``lr_final`` over the steps (piecewise constant per ``chunk`` steps);
         None keeps ``lr``.  ``time_weight``: weight of the 128 arrival-time
         outputs in the squared-error loss relative to the 64 log-probabilities
-        (applied by standardising those targets with std / sqrt(time_weight))."""
+        (applied by standardising those targets with std / sqrt(time_weight)).
+
+        With a ``torch.distributed`` process ``group`` the members are spread
+        over its ranks, one GPU each (rank r trains members r, r + world, ...
+        on ``device``) and every rank returns the whole ensemble (one
+        all_gather of the parameter vectors).  Member k's initialisation and
+        minibatch stream depend on k only, so the ensemble is the same for
+        any number of ranks.  ``member_trainer(k, x, y) -> (params, losses)``
+        replaces the tensor-core trainer (tests)."""
         import math
         import time
-        import torch
         L = np.array([float(box.L[i]) for i in range(3)], np.float64)
         y_mean = targets.mean(0).astype(np.float64)
         y_std = np.maximum(targets.std(0), 1e-6).astype(np.float64)
         y_std[N_CELLS:] /= math.sqrt(time_weight)
         obj = cls(L, y_mean.astype(np.float32), y_std.astype(np.float32), [], z_warp=float(z_warp),
                   z_range=None if z_range is None else (float(z_range[0]), float(z_range[1])))
-        x = torch.from_numpy(obj.normalise(xyz)).to(f"cuda:{device}")
-        y = torch.from_numpy(((targets - y_mean) / y_std).astype(np.float32)).to(f"cuda:{device}")
-        history = []
+        xn = obj.normalise(xyz)
+        yn = ((targets - y_mean) / y_std).astype(np.float32)
+        if member_trainer is None:
+            import torch
+            x = torch.from_numpy(xn).to(f"cuda:{device}")
+            y = torch.from_numpy(yn).to(f"cuda:{device}")
+
+            def member_trainer(k, x, y):
+                net = MLP(device, max_batch=batch, seed=seed * 1000 + k)
+                try:
+                    net.set_data(x, y)
+                    hist = []
+                    for s0 in range(0, steps, chunk):
+                        ns = min(chunk, steps - s0)
+                        if lr_final is None:
+                            lr_now = lr
+                        else:
+                            mid = (s0 + 0.5 * ns) / steps
+                            lr_now = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * mid))
+                        hist.append(net.train(ns, batch=batch, lr=lr_now, seed=seed * 1000 + k))
+                        if log and ((s0 + ns) % 2000 == 0 or s0 + ns == steps):
+                            log(f"member {k} step {s0 + ns}: lr {lr_now:.2e} loss {hist[-1]:.5f}")
+                    return net.get_params(), hist
+                finally:
+                    net.close()
+        else:
+            x, y = xn, yn
+        rank, world = 0, 1
+        if group is not None:
+            import torch.distributed as dist
+            rank, world = dist.get_rank(group), dist.get_world_size(group)
+        mine = members_of_rank(members, rank, world)
         t0 = time.perf_counter()
-        for k in range(members):
-            net = MLP(device, max_batch=batch, seed=seed * 1000 + k)
-            net.set_data(x, y)
-            hist = []
-            for s0 in range(0, steps, chunk):
-                ns = min(chunk, steps - s0)
-                if lr_final is None:
-                    lr_now = lr
-                else:
-                    mid = (s0 + 0.5 * ns) / steps
-                    lr_now = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * mid))
-                hist.append(net.train(ns, batch=batch, lr=lr_now, seed=seed * 1000 + k))
-                if log and ((s0 + ns) % 2000 == 0 or s0 + ns == steps):
-                    log(f"member {k} step {s0 + ns}: lr {lr_now:.2e} loss {hist[-1]:.5f}")
-            obj.members.append(net.get_params())
-            history.append(hist)
-            net.close()
+        trained = {k: member_trainer(k, x, y) for k in mine}
+        if group is None:
+            params = [trained[k][0] for k in range(members)]
+            history = [trained[k][1] for k in range(members)]
+        else:
+            params, history = _gather_members(trained, members, world, group)
+        obj.members = [np.asarray(p, np.float32) for p in params]
         obj.meta = {"steps": steps, "batch": batch, "lr": lr, "lr_final": lr_final,
                     "time_weight": time_weight, "z_warp": z_warp, "z_range": obj.z_range, "seed": seed,
-                    "train_seconds": time.perf_counter() - t0, "loss_history": history}
+                    "train_seconds": time.perf_counter() - t0, "loss_history": history,
+                    "ranks": world}
         return obj
 
     def raw_outputs(self, xyz: np.ndarray, device: int = 0):

@@ -89,6 +89,30 @@ def rel_error(p_pred: np.ndarray, p_true: np.ndarray, photons: int, min_counts: 
             "cells": int(m.sum())}
 
 
+def scan_light_sharded(engine, box, op, ro, pts: np.ndarray, photons: int, seed: int, group):
+    """scan_light over the ranks of ``group``: rank r scans a contiguous range
+    of the points with the photon ids the single-GPU scan gives them
+    (pid_offset = points before x photons), and every rank gets the whole
+    result (the same as one GPU's scan)."""
+    import torch.distributed as dist
+    from .sharding import photon_range
+    from .surrogate import ScanResult, scan_light
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    p0, n = photon_range(pts.shape[0], rank, world)
+    part = scan_light(engine, box, op, ro, points=pts[p0:p0 + n], photons_per_point=photons, seed=seed,
+                      pid_offset=p0 * photons) if n else None
+    parts = [None] * world
+    dist.all_gather_object(parts, (p0, part), group=group)
+    parts = sorted((p for p in parts if p[1] is not None), key=lambda p: p[0])
+    cat = lambda f: np.concatenate([getattr(p[1], f) for p in parts], axis=0)
+    counters = {}
+    for _, r in parts:
+        for k, v in r.counters.items():
+            counters[k] = counters.get(k, 0) + v
+    return ScanResult(pts, photons, cat("counts"), cat("tsum"), cat("tsum2"), cat("tmin"), counters,
+                      max(r.seconds for _, r in parts))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--setup", choices=sorted(SETUPS), default="bgo_esr")
@@ -122,7 +146,21 @@ def main(argv=None):
 
     from .surrogate import LightSurrogate, grid_points, light_targets, scan_light, split_holdout
     from .transport import Engine
+    import os
 
+    # under torchrun: one process per GPU; the scan points and the ensemble
+    # members are spread over the ranks, rank 0 validates and saves
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    group = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        args.device = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(args.device)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        group = dist.group.WORLD
     box, op, ro = setup(args.setup)
     eng = Engine(args.device)
     rep = {"setup": args.setup, "grid": list(args.grid), "photons_per_point": args.photons,
@@ -130,7 +168,10 @@ def main(argv=None):
            "lr_final": args.lr_final, "time_weight": args.time_weight, "z_warp": args.z_warp,
            "z_range": args.z_range}
     pts = grid_points(box, tuple(args.grid), z_warp=args.z_warp, z_range=args.z_range)
-    scan = scan_light(eng, box, op, ro, points=pts, photons_per_point=args.photons, seed=args.seed)
+    if group is None:
+        scan = scan_light(eng, box, op, ro, points=pts, photons_per_point=args.photons, seed=args.seed)
+    else:
+        scan = scan_light_sharded(eng, box, op, ro, pts, args.photons, args.seed, group)
     n_ph = pts.shape[0] * args.photons
     rep["scan"] = {"points": int(pts.shape[0]), "photons": n_ph, "seconds": scan.seconds,
                    "photons_per_s": n_ph / scan.seconds, "detected_fraction": scan.counters["ndet"] / n_ph}
@@ -146,12 +187,17 @@ def main(argv=None):
                                    lr_final=args.lr_final if args.lr_final >= 0 else None,
                                    time_weight=args.time_weight, z_warp=args.z_warp,
                                    z_range=args.z_range, seed=args.seed,
-                                   device=args.device,
+                                   device=args.device, group=group,
                                    log=lambda s: print(s, flush=True))
         rep["train_seconds"] = sur.meta["train_seconds"]
         rep["final_loss"] = [h[-1] for h in sur.meta["loss_history"]]
         print(f"training: {sur.meta['train_seconds']:.1f} s", flush=True)
 
+    if rank != 0:
+        eng.close()
+        import torch.distributed as dist
+        dist.destroy_process_group()
+        return rep
     # held-out validation against a high-statistics truth
     rng = np.random.default_rng(5)
     sub = np.sort(rng.choice(ho, size=min(args.truth_points, ho.size), replace=False))
@@ -219,6 +265,9 @@ def main(argv=None):
             with open(args.report, "w") as f:
                 json.dump(rep, f, indent=1)
         eng.close()
+        if group is not None:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return rep
     sur.meta.update({"setup": args.setup, "grid": list(args.grid), "photons_per_point": args.photons,
                      "z_range": args.z_range})
@@ -227,6 +276,9 @@ def main(argv=None):
         with open(args.report, "w") as f:
             json.dump(rep, f, indent=1)
     eng.close()
+    if group is not None:
+        import torch.distributed as dist
+        dist.destroy_process_group()
     return rep
 
 

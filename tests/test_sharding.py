@@ -153,3 +153,58 @@ def test_shard_plans_cover_the_sources_once():
         check_segments([1, 2], [1, 0], 2)
     with pytest.raises(ValueError):
         check_segments([1, -2], [0, 1], 2)
+
+
+def _fake_trainer(calls):
+    def train(k, x, y):
+        calls.append(k)
+        # a deterministic function of the member index and of the data
+        p = (np.arange(181_952, dtype=np.float32) % 97) * np.float32(k + 1) + np.float32(float(x.sum()))
+        return p, [float(k), float(k) + 0.5, float(y.mean())]
+    return train
+
+
+def _surrogate_data():
+    from crysplight_b200.params import Box
+    from crysplight_b200.surrogate import grid_points
+    box = Box((48.0, 48.0, 22.4))
+    pts = grid_points(box, (4, 4, 3))
+    rng = np.random.default_rng(3)
+    return box, pts, rng.normal(size=(pts.shape[0], 192)).astype(np.float32)
+
+
+def _member_worker(rank, world, port, outdir):
+    import torch.distributed as dist
+    from crysplight_b200.surrogate import LightSurrogate
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        box, pts, y = _surrogate_data()
+        calls = []
+        sur = LightSurrogate.train(box, pts, y, members=5, group=dist.group.WORLD,
+                                   member_trainer=_fake_trainer(calls))
+        np.savez(os.path.join(outdir, f"m{rank}.npz"), members=np.stack(sur.members),
+                 calls=np.array(calls), hist=np.array(sur.meta["loss_history"]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_surrogate_members_one_per_rank(tmp_path):
+    """Ensemble members spread over two gloo ranks (rank r trains members r,
+    r + 2, ...) and gathered: every rank holds the same ensemble, in member
+    order, as one process training all five."""
+    import torch.multiprocessing as mp
+    from crysplight_b200.surrogate import LightSurrogate, members_of_rank
+    assert members_of_rank(5, 0, 2) == [0, 2, 4] and members_of_rank(5, 1, 2) == [1, 3]
+    assert members_of_rank(3, 3, 4) == []
+    mp.spawn(_member_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    box, pts, y = _surrogate_data()
+    calls = []
+    ref = LightSurrogate.train(box, pts, y, members=5, member_trainer=_fake_trainer(calls))
+    assert calls == [0, 1, 2, 3, 4]
+    for r in range(2):
+        got = dict(np.load(tmp_path / f"m{r}.npz"))
+        assert got["calls"].tolist() == members_of_rank(5, r, 2)
+        assert np.array_equal(got["members"], np.stack(ref.members))
+        assert np.allclose(got["hist"], np.array(ref.meta["loss_history"]))
