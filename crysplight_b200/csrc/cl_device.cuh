@@ -59,9 +59,12 @@ __device__ __forceinline__ uint4 philox4x32_10_rk(uint4 c, const uint32_t* __res
 }
 
 // randu, src/philox.jl:62: ((x >>> 8) + 1.0f0) * 2^-24, exact, in (0, 1].
+// (x >> 8) < 2^24 converts exactly, and (f + 1) * 2^-24 = f * 2^-24 + 2^-24 is
+// representable, so one fused multiply-add gives the same bits as the
+// reference's add then multiply (neither rounds).
 __device__ __forceinline__ float u32_to_randu(uint32_t x)
 {
-    return __fmul_rn(__fadd_rn((float)(x >> 8), 1.0f), 0x1p-24f);
+    return __fmaf_rn((float)(x >> 8), 0x1p-24f, 0x1p-24f);
 }
 
 // A photon's uniform stream (PhiloxStream, src/philox.jl:34-62): key = seed,
@@ -123,6 +126,21 @@ __device__ __forceinline__ void rng_fill(Rng& r, float* ring, const uint32_t* rk
         o[b] = philox4x32_10_rk(make_uint4(r.pid_lo, r.pid_hi, r.block + (uint32_t)b, 0u), rk);
     r.block += (uint32_t)NB;
     const uint32_t w = r.head + (uint32_t)r.cnt;
+    if (RING_LEN % (4 * NB) == 0 && (RING_LEN & (RING_LEN - 1)) == 0) {
+        // every fill writes 4*NB words and pops move head and cnt in step, so
+        // the write position head + cnt stays a multiple of 4*NB: the block
+        // never wraps and its stores sit at fixed offsets from its first word
+        float* blk = ring + (size_t)(w & (uint32_t)(RING_LEN - 1)) * RING_STRIDE;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            blk[(4 * b + 0) * RING_STRIDE] = u32_to_randu(o[b].x);
+            blk[(4 * b + 1) * RING_STRIDE] = u32_to_randu(o[b].y);
+            blk[(4 * b + 2) * RING_STRIDE] = u32_to_randu(o[b].z);
+            blk[(4 * b + 3) * RING_STRIDE] = u32_to_randu(o[b].w);
+        }
+        r.cnt += 4 * NB;
+        return;
+    }
 #if CL_RING_WRAP
     // w < 2 RING_LEN: one conditional subtraction wraps each index
     auto at = [&](uint32_t k) -> float& {

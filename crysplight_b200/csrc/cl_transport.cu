@@ -561,8 +561,12 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
             if (MODE == 0) {
                 const int32_t slot = cell + A.cells * time_bin0(t, P);
                 const unsigned g = __match_any_sync(dmask, slot);
-                if (lane == __ffs(g) - 1) atomicAdd(tile_counts + slot, (uint32_t)__popc(g));
-                atomicMin(tile_keys + cell, key);
+                // one atomic per distinct slot: the group's count and its earliest time
+                const uint32_t kmin = __reduce_min_sync(g, key);
+                if (lane == __ffs(g) - 1) {
+                    atomicAdd(tile_counts + slot, (uint32_t)__popc(g));
+                    atomicMin(tile_keys + cell, kmin);
+                }
             } else {
                 // a segment id outside the maps (untrusted device input) drops the detection
                 const bool seg_ok = seg >= 0 && (int64_t)seg < A.n_seg;
@@ -571,8 +575,11 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
                     const unsigned long long slot =
                         (unsigned long long)seg * (unsigned long long)A.cells + (unsigned long long)cell;
                     const unsigned g = __match_any_sync(okmask, slot);
-                    if (lane == __ffs(g) - 1) atomicAdd(A.maps + slot, (uint32_t)__popc(g));
-                    atomicMin(A.keys + slot, key);
+                    const uint32_t kmin = __reduce_min_sync(g, key);
+                    if (lane == __ffs(g) - 1) {
+                        atomicAdd(A.maps + slot, (uint32_t)__popc(g));
+                        atomicMin(A.keys + slot, kmin);
+                    }
                     if (MODE == 2) {
                         // fixed-point time moments (exact integer sums, order-independent)
                         const float tc = fminf(fmaxf(t, 0.0f), CL_MOMENT_T_MAX_NS);
