@@ -104,7 +104,7 @@ def test_sincos_facet_angles(engine, oracle):
         ref = oracle.eval_math(fn, a)
         nbad = int((dev.view(np.uint32) != ref.view(np.uint32)).sum())
         print(fn, "mismatches:", nbad, "of", a.size)
-        assert nbad <= a.size * 1e-6
+        assert nbad == 0
 
 
 def test_math_special_values(engine, oracle):
