@@ -298,22 +298,41 @@ __device__ __forceinline__ float cl_logf_u(float x, const double2* __restrict__ 
 // recombined as S + (S (cos r - 1) + C sin r) and C + (C (cos r - 1) - S sin r).
 // The table-driven core for 0 <= x <= 1e4 (the transport passes azimuths
 // 2*pi*u in (0, 2*pi] and facet tilts in [0, 1.2)); +0 maps to (+0, 1).
+// The core's Float64 constants sit in the constant bank, so every Float64
+// instruction takes its coefficient as an operand (a 64-bit immediate cannot
+// be encoded and would first be moved into registers).
+static __constant__ double c_sc_coef[10] = {CLM_SC_INV_DELTA, CLM_SC_DELTA_HI, CLM_SC_DELTA_LO, CLM_TS7,
+                                            CLM_TS5, CLM_TS3, CLM_TC8, CLM_TC6, CLM_TC4, CLM_TC2};
+#ifndef CL_SC_MAGIC_RINT
+#define CL_SC_MAGIC_RINT 1
+#endif
+
 template <int STRIDE = 1>
 __device__ __forceinline__ void cl_sincosf_core(float x, const double2* __restrict__ sctab,
                                                 float* sp, float* cp)
 {
     const double xd = (double)x;
-    const double n = rint(xd * CLM_SC_INV_DELTA);
-    double r = fma(-n, CLM_SC_DELTA_HI, xd);
-    r = fma(-n, CLM_SC_DELTA_LO, r);
-    const double2 sc = sctab[((int)n & (CLM_SC_N - 1)) * STRIDE];
+#if CL_SC_MAGIC_RINT
+    // rint by the 1.5*2^52 shift (round to nearest even, |q| < 2^51): the
+    // integer sits in the low word of the shifted sum
+    const double q = xd * c_sc_coef[0];
+    const double sh = q + 0x1.8p52;
+    const double n = sh - 0x1.8p52;
+    const int ni = __double2loint(sh);
+#else
+    const double n = rint(xd * c_sc_coef[0]);
+    const int ni = (int)n;
+#endif
+    double r = fma(-n, c_sc_coef[1], xd);
+    r = fma(-n, c_sc_coef[2], r);
+    const double2 sc = sctab[(ni & (CLM_SC_N - 1)) * STRIDE];
     const double r2 = r * r;
-    double ps = fma(CLM_TS7, r2, CLM_TS5);
-    ps = fma(ps, r2, CLM_TS3);
+    double ps = fma(c_sc_coef[3], r2, c_sc_coef[4]);
+    ps = fma(ps, r2, c_sc_coef[5]);
     const double sr = fma(r * r2, ps, r);
-    double pc = fma(CLM_TC8, r2, CLM_TC6);
-    pc = fma(pc, r2, CLM_TC4);
-    pc = fma(pc, r2, CLM_TC2);
+    double pc = fma(c_sc_coef[6], r2, c_sc_coef[7]);
+    pc = fma(pc, r2, c_sc_coef[8]);
+    pc = fma(pc, r2, c_sc_coef[9]);
     const double cm1 = r2 * pc;
     *sp = __double2float_rn(sc.x + fma(sc.x, cm1, sc.y * sr));
     *cp = __double2float_rn(sc.y + fma(sc.y, cm1, -(sc.x * sr)));

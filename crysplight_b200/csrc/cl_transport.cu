@@ -181,7 +181,14 @@ enum : int32_t { FK_NONE = 0, FK_READOUT = 1, FK_POLISHED = 2, FK_FACET = 3 };
 #define CL_MIN_CTAS_PER_SM 4
 #endif
 
-template <int MODE, bool REC, bool TILE>
+// Optical configurations compiled with their flags as constants (the branches
+// they rule out vanish from the loop): SPEC_ESR and SPEC_TEFLON are a rough
+// (UNIFIED) back-painted wrap, specular or Lambertian, over a full, one-sided
+// readout face with finite absorption and Rayleigh lengths -- the BGO+ESR and
+// CsI(Tl)+Teflon run files; SPEC_ANY reads every flag from the parameters.
+enum : int { SPEC_ANY = 0, SPEC_ESR = 1, SPEC_TEFLON = 2 };
+
+template <int MODE, bool REC, bool TILE, int SPEC>
 __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(const __grid_constant__ KArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -211,7 +218,13 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
     const unsigned lt_mask = (1u << lane) - 1u;
     const double2* my_tab = s_tab + (lane % LOG_COPIES);
     const double2* my_sctab = s_sctab + (lane % SC_COPIES);
-    const bool uni_possible = P.air_gap && P.sigma_alpha > 0.0f;
+    const bool air_gap = SPEC != SPEC_ANY || P.air_gap;
+    const bool uni_possible = SPEC != SPEC_ANY || (P.air_gap && P.sigma_alpha > 0.0f);
+    const bool wrap_specular = SPEC == SPEC_ESR || (SPEC == SPEC_ANY && P.wrap_specular);
+    const bool abs_finite = SPEC != SPEC_ANY || P.abs_finite;
+    const bool ray_finite = SPEC != SPEC_ANY || P.ray_finite;
+    const bool disc = SPEC == SPEC_ANY && P.disc;
+    const bool two_sided = SPEC == SPEC_ANY && P.two_sided;
     const float inf = __int_as_float(0x7f800000);
 
     // per-lane photon state
@@ -321,8 +334,8 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
             if (P.tau > 0.0f) { a0 = rng_pop(rng, ring); nl0 = true; }
         } else if (st == S_MOVE || st == S_UNI) {
             if (st == S_MOVE) {
-                if (P.abs_finite) { a0 = rng_pop(rng, ring); nl0 = true; }
-                if (P.ray_finite) { a1 = rng_pop(rng, ring); nl1 = true; }
+                if (abs_finite) { a0 = rng_pop(rng, ring); nl0 = true; }
+                if (ray_finite) { a1 = rng_pop(rng, ring); nl1 = true; }
             }
             if (uni_possible) {
                 // speculative: the next three uniforms are the UNIFIED try's
@@ -375,8 +388,8 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
         } else if (st == S_MOVE) {
             float d;
             const int32_t f = wall_hit(P, x, y, z, ux, uy, uz, d);
-            const float d_abs = P.abs_finite ? (-P.abs_len) * L0 : inf;
-            const float d_ray = P.ray_finite ? (-P.ray_len) * L1 : inf;
+            const float d_abs = abs_finite ? (-P.abs_len) * L0 : inf;
+            const float d_ray = ray_finite ? (-P.ray_len) * L1 : inf;
             if (d_abs < d && d_abs <= d_ray) {
                 status = ST_ABS_BULK;
             } else if (d_ray < d) {
@@ -397,18 +410,18 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
                 t += d * P.inv_v;
                 const float cosi = a == 1 ? fabsf(ux) : (a == 2 ? fabsf(uy) : fabsf(uz));
                 face = f;
-                if (f == FACE_BACK || (P.two_sided && f == FACE_FRONT)) {
+                if (f == FACE_BACK || (two_sided && f == FACE_FRONT)) {
                     // readout face, src/transport.jl:161-185: Fresnel below
                     fk = FK_READOUT; fn2 = P.n_coupling; fq2 = P.qc2; fcos = cosi;
-                } else if (!P.air_gap) {
+                } else if (!air_gap) {
                     // front-painted wrap, src/transport.jl:186-198
                     if (rng_pop(rng, ring) <= P.wrap_R) {
-                        if (P.wrap_specular) { specular(ux, uy, uz, f); wall_done = true; }
+                        if (wrap_specular) { specular(ux, uy, uz, f); wall_done = true; }
                         else st = S_LAMB;
                     } else {
                         status = ST_ABS_WALL;
                     }
-                } else if (P.sigma_alpha > 0.0f) {
+                } else if (uni_possible) {
                     tries = 0;
                     uni = true;                      // UNIFIED lobe, below
                 } else {
@@ -481,7 +494,7 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
                 if (refl) {
                     specular(ux, uy, uz, face);
                     wall_done = true;
-                } else if (!P.disc || (x - P.cx) * (x - P.cx) + (y - P.cy) * (y - P.cy) <= P.r2) {
+                } else if (!disc || (x - P.cx) * (x - P.cx) + (y - P.cy) * (y - P.cy) <= P.r2) {
                     if (rng_pop(rng, ring) <= P.pde) {
                         int32_t ii = 1 + (int32_t)(x / P.pitch);
                         int32_t jj = 1 + (int32_t)(y / P.pitch);
@@ -535,7 +548,7 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
         // transmitted into the air gap: the reflector (src/transport.jl:214-225)
         if (to_wrap) {
             if (rng_pop(rng, ring) <= P.wrap_R) {
-                if (P.wrap_specular) { specular(ux, uy, uz, face); wall_done = true; }
+                if (wrap_specular) { specular(ux, uy, uz, face); wall_done = true; }
                 else st = S_LAMB;
             } else {
                 status = ST_ABS_WALL;
@@ -828,13 +841,21 @@ static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Allow dynamic shared memory up to the opt-in limit minus the kernel's
 // static shared memory (their sum may not exceed the limit).
+template <int MODE, bool REC, bool TILE, int SPEC>
+static void set_kernel_attrs_spec(int smem_optin)
+{
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, transport_kernel<MODE, REC, TILE, SPEC>) != cudaSuccess) return;
+    cudaFuncSetAttribute(transport_kernel<MODE, REC, TILE, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         smem_optin - (int)fa.sharedSizeBytes);
+}
+
 template <int MODE, bool REC, bool TILE>
 static void set_kernel_attrs(int smem_optin)
 {
-    cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, transport_kernel<MODE, REC, TILE>) != cudaSuccess) return;
-    cudaFuncSetAttribute(transport_kernel<MODE, REC, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         smem_optin - (int)fa.sharedSizeBytes);
+    set_kernel_attrs_spec<MODE, REC, TILE, SPEC_ANY>(smem_optin);
+    set_kernel_attrs_spec<MODE, REC, TILE, SPEC_ESR>(smem_optin);
+    set_kernel_attrs_spec<MODE, REC, TILE, SPEC_TEFLON>(smem_optin);
 }
 
 extern "C" {
@@ -1028,10 +1049,18 @@ static Scratch scratch_of(cl_handle* h)
     return s;
 }
 
-template <int MODE, bool REC, bool TILE>
-static int launch_transport(cl_handle* h, const KArgs& a, size_t smem, cudaStream_t st)
+// The compiled configuration a launch can use (SPEC_ANY where none matches).
+static int spec_of(const Physics& P)
 {
-    auto kern = transport_kernel<MODE, REC, TILE>;
+    if (!P.air_gap || !(P.sigma_alpha > 0.0f) || P.disc || P.two_sided || !P.abs_finite || !P.ray_finite)
+        return SPEC_ANY;
+    return P.wrap_specular ? SPEC_ESR : SPEC_TEFLON;
+}
+
+template <int MODE, bool REC, bool TILE, int SPEC>
+static int launch_transport_spec(cl_handle* h, const KArgs& a, size_t smem, cudaStream_t st)
+{
+    auto kern = transport_kernel<MODE, REC, TILE, SPEC>;
     int per_sm = 0;
     CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, h->threads, smem), "occupancy");
     if (per_sm < 1) return set_err(h, CL_ERR_ARG, "transport kernel does not fit on an SM (shared tile too large)");
@@ -1054,6 +1083,16 @@ static int launch_transport(cl_handle* h, const KArgs& a, size_t smem, cudaStrea
     kern<<<(unsigned)grid, h->threads, smem, st>>>(b);
     CK(h, cudaGetLastError(), "transport kernel launch");
     return CL_OK;
+}
+
+template <int MODE, bool REC, bool TILE>
+static int launch_transport(cl_handle* h, const KArgs& a, size_t smem, cudaStream_t st)
+{
+    switch (spec_of(a.P)) {
+    case SPEC_ESR: return launch_transport_spec<MODE, REC, TILE, SPEC_ESR>(h, a, smem, st);
+    case SPEC_TEFLON: return launch_transport_spec<MODE, REC, TILE, SPEC_TEFLON>(h, a, smem, st);
+    default: return launch_transport_spec<MODE, REC, TILE, SPEC_ANY>(h, a, smem, st);
+    }
 }
 
 static int enqueue_point(cl_handle* h, const Physics& P, const float* px, const float* py,
