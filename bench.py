@@ -53,15 +53,18 @@ OPS_PER_STEP = {"scan256": 165.6, "point1m": 186.7}
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per photon-step of the transport kernel, from one
 # ncu capture of each workload at a reduced size (scan: 20,000 photons per
-# point, 3.00 GB for 494.8M photon-steps), scaled to a full launch by its
-# photon-steps.  Almost all of it is L2 misses of the 64 MB log table (about 2
+# point, 3.00 GB for 494.8M photon-steps; point source: the whole 10^6-photon
+# launch, 143 MB for 12.33M photon-steps, mostly the table's first touches),
+# scaled to a full launch by its photon-steps.  Almost all of it is L2 misses of the 64 MB log table (about 2
 # bytes per photon-step and lookup), which grow in proportion to the steps;
 # the sources, offsets and maps are 0.24 MB.
-TRAFFIC_PER_STEP = {"scan256": (2.993991e9 + 6.48064e6) / 494_804_727, "point1m": None}
+TRAFFIC_PER_STEP = {"scan256": (2.991796e9 + 6.923776e6) / 494_804_727,
+                    "point1m": (139.331584e6 + 3.77856e6) / 12_332_791}
 # Warp instructions the transport kernel issues per photon-step (smsp__inst_executed
-# of the same ncu capture: 17.23 G for 494.8M photon-steps); with the live
-# steps/s this gives the kernel's issue rate against the SMs' issue slots.
-WARP_INST_PER_STEP = {"scan256": 17228482017 / 494_804_727}
+# of the same ncu captures: 15.81 G for 494.8M photon-steps on the scan, 0.78 G
+# for 12.33M on the point source); with the live steps/s this gives the
+# kernel's issue rate against the SMs' issue slots.
+WARP_INST_PER_STEP = {"scan256": 15_809_711_771 / 494_804_727, "point1m": 779_417_179 / 12_332_791}
 
 
 def events_workload(n_events: int = 50_000):
@@ -163,6 +166,7 @@ def surrogate_training_bench(dev, steps: int = 200, warmup: int = 20) -> dict:
     peak = measured_peaks().get("bf16_tflops_sustained", 1400.0)
     return {"metric": "surrogate training steps/s", "batch": 65536, "ms_per_step": dt * 1e3,
             "tflops": flop / dt / 1e12, "peak_tflops": peak, "frac": flop / dt / 1e12 / peak,
+            "peak_source": measured_peaks().get("source", "measured"),
             "note": "one cl_mlp_train call of all steps (host time around a synchronised loop)"}
 
 
@@ -189,7 +193,7 @@ def surrogate_events_workload(n_events: int = 500_000):
 
 
 def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wall_min_mm=1.0,
-                               expert: bool = True):
+                               expert: bool = True, expert_files=None):
     """events/s of the surrogate + fallback pipeline with the deposits in HBM
     (value), the plain Monte Carlo on the same deposits, their agreement, and
     the whole public call SurrogateEvents.run_events (e2e)."""
@@ -198,7 +202,8 @@ def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wal
     from crysplight_b200.fast_events import SurrogateEvents, compare_maps, photopeak
     from crysplight_b200.surrogate import LightSurrogate
     sur = LightSurrogate.load(SURROGATE_BGO)
-    experts = [LightSurrogate.load(SURROGATE_BGO_FACE)] if expert and os.path.exists(SURROGATE_BGO_FACE) else []
+    files = expert_files if expert_files else ([SURROGATE_BGO_FACE] if os.path.exists(SURROGATE_BGO_FACE) else [])
+    experts = [LightSurrogate.load(f) for f in files] if expert else []
     se = SurrogateEvents(sur, eng, device=dev.index or 0, experts=experts)
     g = gamma_stage(E["mat"], E["box"], n_events=E["n_events"], seed=E["seed"],
                     yield_per_mev=E["yield_"])
@@ -390,11 +395,16 @@ class ClockSampler:
 
 
 def measured_peaks() -> dict:
+    """MEASURED_PEAKS.json (measured on this pool's B200s), else the earlier
+    measurement the profiling notes give as the fallback (marked)."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return json.load(f)
+            d = json.load(f)
+        d.setdefault("source", "measured")
+        return d
     except Exception:
-        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "fallback": True}
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+                "sm_max_mhz": 1965.0, "source": "fallback"}
 
 
 # ------------------------------------------------------------------------------------
@@ -439,8 +449,13 @@ def cpu_sample_desc(W, per: int, dt: float) -> str:
 def cpu_baseline(W, target_s: float) -> dict:
     per = cpu_sample_size(W, target_s)
     dt, n, steps = cpu_run(W, per)
+    reps = 1
+    while dt < 0.5 * target_s:          # the whole workload is shorter than the target: repeat it
+        d2, n2, s2 = cpu_run(W, per)
+        dt, n, steps, reps = dt + d2, n + n2, steps + s2, reps + 1
+    sample = cpu_sample_desc(W, per, dt) + (f", {reps} runs" if reps > 1 else "")
     return {"value": n / dt, "unit": "photons/s", "cores": os.cpu_count(), "kind": "port",
-            "photon_steps_per_s": steps / dt, "sample": cpu_sample_desc(W, per, dt)}
+            "photon_steps_per_s": steps / dt, "sample": sample}
 
 
 def workload_config(W) -> dict:
@@ -606,6 +621,7 @@ def roofline(W, steps_per_launch: int, launch_s: float, in_bytes: int, out_bytes
     return {
         "bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gop/s",
         "frac": achieved / peak, "traffic": traffic, "ops_per_step": ops_step,
+        "peak_source": peaks.get("source", "measured"),
         "note": ("reference Float32/int ops per photon-step x steps / launch time, against "
                  "one op per lane per clock (SMs x 128 lanes x max SM clock of measured)"),
         "hbm": {"achieved": dram / launch_s / 1e9, "peak": hbm_peak, "unit": "GB/s",
@@ -654,10 +670,12 @@ def run_cuda_arm(args, W, rank, world, local_rank):
     if W["name"] == "scan256" and args.point1m:
         # config 1 at its stated size: 10^6 CsI(Tl)+Teflon photons from the centre
         P = workload("point1m")
-        rp = measure_photons(eng, P, max(args.steps, 10), args.warmup, dev, stream)
-        ls = rp["tot_ms"] * 1e-3 / max(args.steps, 10)
-        obj = {"metric": "photons/s", "workload": P["desc"], "unit": "photons/s",
-               "value": P["n"] / ls, "e2e": {"value": P["n"] * max(args.steps, 10) / rp["e2e_s"],
+        # a 1.2 ms launch: 25x the steps, so the clock sampler sees the timed region
+        psteps = 25 * args.steps
+        rp = measure_photons(eng, P, psteps, args.warmup, dev, stream)
+        ls = rp["tot_ms"] * 1e-3 / psteps
+        obj = {"metric": "photons/s", "workload": P["desc"], "unit": "photons/s", "steps": psteps,
+               "value": P["n"] / ls, "e2e": {"value": P["n"] * psteps / rp["e2e_s"],
                                              "unit": "photons/s", "h2d_bytes_per_step": rp["h2d"],
                                              "d2h_bytes_per_step": rp["d2h"]},
                "ms_per_step": ls * 1e3, "photon_steps_per_launch": rp["steps_per_launch"],
@@ -687,7 +705,7 @@ def run_cuda_arm(args, W, rank, world, local_rank):
         # the plain Monte Carlo
         E = surrogate_events_workload(args.surrogate_events)
         r = run_surrogate_events_bench(eng, E, min(args.steps, 3), args.warmup, dev, stream,
-                                       expert=not args.no_expert)
+                                       expert=not args.no_expert, expert_files=args.experts)
         line["surrogate_events"] = {
             "metric": "511keV events/s", "workload": E["desc"], "unit": "events/s",
             "value": r["value"], "e2e": r["e2e"], "plain_mc": r["mc_value"],
@@ -879,7 +897,8 @@ def run_surrogate_events_arm(args, rank, world, local_rank):
     clocks = ClockSampler(local_rank)
     clocks.start()
     r = run_surrogate_events_bench(eng, E, args.steps, args.warmup, dev, stream,
-                                   wall_min_mm=args.wall_min_mm, expert=not args.no_expert)
+                                   wall_min_mm=args.wall_min_mm, expert=not args.no_expert,
+                                   expert_files=args.experts)
     clk = clocks.stop()
     dev_s, e2e_s = r["dev_s"], E["n_events"] / r["e2e"]
     if world > 1:
@@ -942,6 +961,9 @@ def main():
     ap.add_argument("--no-expert", action="store_true",
                     help="events_bgo_surrogate: the whole-crystal ensemble only, without the "
                          "readout-face expert")
+    ap.add_argument("--experts", nargs="*", default=None,
+                    help="events_bgo_surrogate: depth-slab expert ensembles (.npz), applied in "
+                         "order (default: the shipped readout-face expert)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=256,
