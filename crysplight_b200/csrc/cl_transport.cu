@@ -225,6 +225,9 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
     const bool ray_finite = SPEC != SPEC_ANY || P.ray_finite;
     const bool disc = SPEC == SPEC_ANY && P.disc;
     const bool two_sided = SPEC == SPEC_ANY && P.two_sided;
+    // states and interfaces a configuration never reaches (tests on them compile away)
+    constexpr bool lamb_possible = SPEC != SPEC_ESR;      // Lambertian wrap or surround
+    constexpr bool polished_possible = SPEC == SPEC_ANY;  // back-painted face without roughness
     const float inf = __int_as_float(0x7f800000);
 
     // per-lane photon state
@@ -349,7 +352,7 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
             ray_ok = 2.0f * rng_pop(rng, ring) <= 1.0f + mu * mu;
             carry = mu;
             if (ray_ok) { p1 = TWO_PI_F * rng_pop(rng, ring); ns1 = true; }
-        } else if (st == S_LAMB) {
+        } else if (lamb_possible && st == S_LAMB) {
             carry = rng_pop(rng, ring);                       // u for cos(theta)
             p1 = TWO_PI_F * rng_pop(rng, ring); ns1 = true;
         }
@@ -440,7 +443,7 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
                 if (bounces >= P.max_bounces) status = ST_CAP;
                 else st = S_MOVE;
             }
-        } else if (st == S_LAMB) {
+        } else if (lamb_possible && st == S_LAMB) {
             lambertian_from(face, sqrtf(carry), s1, c1, ux, uy, uz);
             wall_done = true;
         }
@@ -512,7 +515,7 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
                 } else {
                     status = ST_ABS_SUR;
                 }
-            } else if (fk == FK_POLISHED) {
+            } else if (polished_possible && fk == FK_POLISHED) {
                 if (refl) { specular(ux, uy, uz, face); wall_done = true; }
                 else to_wrap = true;
             } else {
