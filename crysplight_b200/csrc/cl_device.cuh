@@ -431,7 +431,10 @@ __device__ __forceinline__ int face_axis(int32_t face) { return face <= 2 ? 1 : 
 __device__ __forceinline__ void specular(float& ux, float& uy, float& uz, int32_t face)
 {
     const int a = face_axis(face);
-    if (a == 1) ux = -ux; else if (a == 2) uy = -uy; else uz = -uz;
+    // selects, not branches: a warp whose lanes hit different axes runs one path
+    ux = a == 1 ? -ux : ux;
+    uy = a == 2 ? -uy : uy;
+    uz = a == 3 ? -uz : uz;
 }
 
 // Distance along one axis to the face the direction points at:

@@ -796,6 +796,7 @@ struct cl_handle {
     int warp_chunk = CL_DEFAULT_WARP_CHUNK;   // 0: automatic per launch
     int64_t last_steps = 0;
     int max_smem_optin = 0;
+    int max_smem_per_sm = 0;
     unsigned long long budget_ns = (unsigned long long)(CL_DEFAULT_TIME_BUDGET_S * 1e9);
 };
 
@@ -892,6 +893,8 @@ int cl_create(cl_handle** out, int device)
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess)
         e = cudaDeviceGetAttribute(&h->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&h->max_smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1129,7 +1132,14 @@ static int enqueue_point(cl_handle* h, const Physics& P, const float* px, const 
     a.budget_ns = h->budget_ns;
     const size_t tile_bytes = ((size_t)n_counts + cells) * sizeof(uint32_t);
     const size_t base_bytes = LOGTAB_BYTES + (size_t)RING_LEN * RING_STRIDE * sizeof(float);
-    const bool tile = base_bytes + tile_bytes <= (size_t)std::min(h->max_smem_optin, 160 * 1024);
+    // the shared-memory histogram tile only where it still leaves room for 4
+    // CTAs per SM: with fewer resident warps the loop issues less often, which
+    // costs more than the tile saves in global atomics (10^6-photon point
+    // source, 8x8x81 bins: 879 M photons/s on global atomics at 4 CTAs/SM,
+    // 843 M with the tile at 3)
+    const size_t per_cta = base_bytes + tile_bytes + 1024;
+    const bool tile = base_bytes + tile_bytes <= (size_t)std::min(h->max_smem_optin, 160 * 1024) &&
+                      4 * per_cta <= (size_t)h->max_smem_per_sm;
     const size_t smem = base_bytes + (tile ? tile_bytes : 0);
     if (tile) return want_rec ? launch_transport<0, true, true>(h, a, smem, st)
                               : launch_transport<0, false, true>(h, a, smem, st);
@@ -1573,6 +1583,7 @@ struct NoallocDevice {
     unsigned char* base = nullptr;   // device address of g_noalloc_scratch on this device
     int num_sms = 0;
     int max_smem_optin = 0;
+    int max_smem_per_sm = 0;
 };
 NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
 
@@ -1589,6 +1600,8 @@ int noalloc_setup(int dev, NoallocDevice** out)
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, dev);
         if (e == cudaSuccess)
             e = cudaDeviceGetAttribute(&d.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e == cudaSuccess)
+            e = cudaDeviceGetAttribute(&d.max_smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
         if (e != cudaSuccess) {
             cudaGetLastError();
             snprintf(g_create_err, sizeof g_create_err, "cl_run_photons_noalloc: set-up on device %d: %s",
@@ -1655,6 +1668,7 @@ extern "C" int cl_run_photons_noalloc(const cl_box* box, const cl_optical_params
     tmp.device = dev;
     tmp.num_sms = nd->num_sms;
     tmp.max_smem_optin = nd->max_smem_optin;
+    tmp.max_smem_per_sm = nd->max_smem_per_sm;
     tmp.scratch.p = nd->base;                 // queue / steps / done / err words
     tmp.scratch.cap = b_words;
     unsigned char* base = nd->base;
