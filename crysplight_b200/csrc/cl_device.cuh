@@ -466,14 +466,14 @@ __device__ __forceinline__ void lambertian_from(int32_t face, float ct, float sp
 {
     const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
     const float a = st * cphi, b = st * sphi;
-    switch (face) {
-    case FACE_XP:   ux = -ct; uy = a;   uz = b;   break;
-    case FACE_XM:   ux = ct;  uy = a;   uz = b;   break;
-    case FACE_YP:   ux = a;   uy = -ct; uz = b;   break;
-    case FACE_YM:   ux = a;   uy = ct;  uz = b;   break;
-    case FACE_BACK: ux = a;   uy = b;   uz = -ct; break;
-    default:        ux = a;   uy = b;   uz = ct;  break;
-    }
+    // the inward normal component on the face's axis, (a, b) on the other two
+    // in axis order (XP: (-ct, a, b), YM: (a, ct, b), BACK: (a, b, -ct), ...),
+    // by selects
+    const int ax = face_axis(face);
+    const float n = (face == FACE_XP || face == FACE_YP || face == FACE_BACK) ? -ct : ct;
+    ux = ax == 1 ? n : a;
+    uy = ax == 1 ? a : (ax == 2 ? n : b);
+    uz = ax == 3 ? n : b;
 }
 
 // The tail of rayleigh_dir, src/optics.jl:93-111: rotate u by the polar
