@@ -348,8 +348,15 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
                 p1 = TWO_PI_F * rng_peek(rng, ring, 2u); ns1 = true;
             }
         } else if (st == S_RAY) {
-            const float mu = 1.0f - 2.0f * rng_pop(rng, ring);
+            float mu = 1.0f - 2.0f * rng_pop(rng, ring);
             ray_ok = 2.0f * rng_pop(rng, ring) <= 1.0f + mu * mu;
+            if (!ray_ok) {
+                // a second try in the same iteration (the reference's next
+                // draws, in order): 8 of 9 scatters end in one iteration
+                ++tries;
+                mu = 1.0f - 2.0f * rng_pop(rng, ring);
+                ray_ok = 2.0f * rng_pop(rng, ring) <= 1.0f + mu * mu;
+            }
             carry = mu;
             if (ray_ok) { p1 = TWO_PI_F * rng_pop(rng, ring); ns1 = true; }
         } else if (lamb_possible && st == S_LAMB) {
