@@ -53,18 +53,18 @@ OPS_PER_STEP = {"scan256": 165.6, "point1m": 186.7}
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) per photon-step of the transport kernel, from one
 # ncu capture of each workload at a reduced size (scan: 20,000 photons per
-# point, 3.00 GB for 494.8M photon-steps; point source: the whole 10^6-photon
+# point, 3.01 GB for 494.8M photon-steps; point source: the whole 10^6-photon
 # launch, 143 MB for 12.33M photon-steps, mostly the table's first touches),
 # scaled to a full launch by its photon-steps.  Almost all of it is L2 misses of the 64 MB log table (about 2
 # bytes per photon-step and lookup), which grow in proportion to the steps;
 # the sources, offsets and maps are 0.24 MB.
-TRAFFIC_PER_STEP = {"scan256": (2.991796e9 + 6.923776e6) / 494_804_727,
-                    "point1m": (139.331584e6 + 3.77856e6) / 12_332_791}
+TRAFFIC_PER_STEP = {"scan256": (3.003462e9 + 7.173888e6) / 494_804_727,
+                    "point1m": (139.735552e6 + 3.632384e6) / 12_332_791}
 # Warp instructions the transport kernel issues per photon-step (smsp__inst_executed
-# of the same ncu captures: 15.81 G for 494.8M photon-steps on the scan, 0.78 G
+# of the same ncu captures: 15.42 G for 494.8M photon-steps on the scan, 0.80 G
 # for 12.33M on the point source); with the live steps/s this gives the
 # kernel's issue rate against the SMs' issue slots.
-WARP_INST_PER_STEP = {"scan256": 15_809_711_771 / 494_804_727, "point1m": 779_417_179 / 12_332_791}
+WARP_INST_PER_STEP = {"scan256": 15_422_450_065 / 494_804_727, "point1m": 804_971_827 / 12_332_791}
 
 
 def events_workload(n_events: int = 50_000):
