@@ -639,7 +639,7 @@ def run_cuda_arm(args, W, rank, world, local_rank):
     import crysplight_b200 as cl
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    if world > 1:
+    if world > 1 or args.sharded:
         run_sharded_arm(args, W, rank, world, local_rank)
         return
     eng = cl.Engine(local_rank)
@@ -964,6 +964,9 @@ def main():
     ap.add_argument("--experts", nargs="*", default=None,
                     help="events_bgo_surrogate: depth-slab expert ensembles (.npz), applied in "
                          "order (default: the shipped readout-face expert)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="scan256: the multi-GPU path (sharding.ShardedSegments with NCCL) even on "
+                         "one rank (it is the default for more than one rank)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--points", type=int, default=256,
@@ -996,16 +999,21 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args, W, rank, world)
         return
-    if world > 1:
+    distributed = world > 1 or args.sharded
+    if distributed:
         import datetime
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29531")
+        os.environ.setdefault("RANK", str(rank))
+        os.environ.setdefault("WORLD_SIZE", str(world))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
         run_cuda_arm(args, W, rank, world, local_rank)
     finally:
-        if world > 1:
+        if distributed:
             import torch.distributed as dist
             dist.destroy_process_group()
 
