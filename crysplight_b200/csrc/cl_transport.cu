@@ -150,8 +150,8 @@ enum : int32_t {
     S_LAMB = 5,   // Lambertian re-injection (src/optics.jl:118-138)
 };
 // Uniforms one iteration can consume at most (move: abs, ray, 3 for the
-// UNIFIED try, Fresnel, wrap).  The ring is topped up to this before the
-// iteration's draws.
+// UNIFIED try, Fresnel, wrap; a Rayleigh frame: two tries of 2 and the
+// azimuth).  The ring is topped up to this before the iteration's draws.
 constexpr int DRAWS_PER_ITER = 7;
 // Fresnel interfaces met in an iteration (one evaluation serves all three).
 enum : int32_t { FK_NONE = 0, FK_READOUT = 1, FK_POLISHED = 2, FK_FACET = 3 };
@@ -161,9 +161,6 @@ enum : int32_t { FK_NONE = 0, FK_READOUT = 1, FK_POLISHED = 2, FK_FACET = 3 };
 #endif
 #ifndef CL_FILL_BLOCKS
 #define CL_FILL_BLOCKS 2
-#endif
-#ifndef CL_NEED_BY_STATE
-#define CL_NEED_BY_STATE 0
 #endif
 #ifndef CL_USE_LOGTAB
 #define CL_USE_LOGTAB 1
@@ -308,13 +305,7 @@ __global__ void __launch_bounds__(256, CL_MIN_CTAS_PER_SM) transport_kernel(cons
 
         // ---- top up the uniform ring: one Philox call site for the warp ----
         {
-#if CL_NEED_BY_STATE
-            // the most uniforms this lane's state can consume in one iteration
-            const int need = st == S_MOVE ? DRAWS_PER_ITER : (st == S_UNI ? 5 : (st == S_LAMB ? 2 : 3));
-            const bool want = st != S_IDLE && rng.cnt < need;
-#else
             const bool want = st != S_IDLE && rng.cnt < DRAWS_PER_ITER;
-#endif
             if (__any_sync(FULL, want)) {
 #if CL_FILL_JOIN
                 // every lane with room tops up at this convergent point, so
