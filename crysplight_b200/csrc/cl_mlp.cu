@@ -2,16 +2,21 @@
 // MLP trained and evaluated on sm_100a by hand-written kernels.
 //
 // GEMMs run on the 5th-generation tensor cores: BF16 operands streamed by TMA
-// into a 4-stage shared-memory ring (128-byte swizzled K-major tiles), one
-// thread issuing tcgen05.mma into a double-buffered FP32 accumulator in tensor
-// memory, and four warps draining it through fused epilogues (bias, SiLU,
-// SiLU', the loss and its gradient, bias-gradient column sums, the layer-1
-// gradients, BF16 casts, transposed copies, split-K partials).  The 3-wide
-// input layer, the split-K reduction and Adam run on the CUDA cores.
+// into a 2- to 4-stage shared-memory ring (128-byte swizzled K-major tiles),
+// one thread issuing tcgen05.mma into a double-buffered FP32 accumulator in
+// tensor memory, and sixteen warps draining it through fused epilogues (bias,
+// SiLU, SiLU', the loss and its gradient, bias-gradient column sums, the
+// layer-1 gradients, BF16 casts, transposed copies, split-K partials).  The
+// 3-wide input layer, the split-K reduction and Adam run on the CUDA cores.
 // The epilogues are element-wise work over the 128 x N accumulator of every
 // tile; they are spread over sixteen warps (four per TMEM lane quadrant, each
 // taking every fourth 32-column chunk) so that draining a tile keeps pace
-// with the tensor cores filling the other accumulator.
+// with the tensor cores filling the other accumulator.  Their BF16 outputs
+// (row-major and transposed) are staged in shared memory as 32 x 32 tiles and
+// written by TMA stores: stored straight from registers, each 16-byte store
+// of a warp touched 32 rows, and the store queue, not the arithmetic, set the
+// pace.  The per-column constants they read (biases, the layer-1 weights) are
+// staged in shared memory once per CTA.
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -37,7 +42,6 @@ using bf16 = __nv_bfloat16;
 
 constexpr int TILE_M = 128;     // rows per CTA tile (TMEM lanes)
 constexpr int TILE_K = 64;      // K elements per pipeline stage (one 128-byte swizzle row)
-constexpr int STAGES = 3;       // TMA -> MMA pipeline depth
 #ifndef CL_MLP_EPI_WARPS
 #define CL_MLP_EPI_WARPS 16
 #endif
@@ -48,13 +52,6 @@ constexpr int MMA_WARP = EPI_WARPS + 1;         // MMA issuer / TMEM owner
 constexpr int GEMM_THREADS = 32 * (EPI_WARPS + 2);
 constexpr uint32_t TMEM_COLS = 512; // two 256-column FP32 accumulators
 constexpr uint32_t WAIT_BUDGET = 1u << 22;   // polls before a wait gives up
-constexpr int RED_STRIDE = 33;
-constexpr size_t RED_BYTES = (size_t)EPI_WARPS * (32 * RED_STRIDE + 32 * 3) * sizeof(float);
-
-__host__ __device__ constexpr size_t gemm_smem_bytes(int N)
-{
-    return 1024 + (size_t)STAGES * ((size_t)TILE_M * 128 + (size_t)N * 128) + RED_BYTES;
-}
 
 enum Epi : int {
     EPI_F32 = 0,         // out_f[m][n] = acc
@@ -65,6 +62,30 @@ enum Epi : int {
     EPI_LOSS = 5,        // o = acc + b, d = o - target: loss += scale d^2, g = bf16(2 scale d) -> out_h, out_ht, colsum
     EPI_DSILU_L1 = 6,    // as EPI_DSILU with zprev recomputed from x, W1, b1; colsum and gw1 += g, g x
 };
+
+// Per epilogue: the BF16 tiles each epilogue warp stages in shared memory per
+// 32 x 32 chunk (2 KB each, written out by TMA stores; the transposed tile
+// also feeds the column sums), the TMA -> MMA pipeline depth that leaves room
+// for them (48 KB per stage for N = 256), and the per-column constants staged
+// in shared memory (bias; for EPI_DSILU_L1 also W1 by input component).
+template <int EPI>
+struct EpiCfg {
+    static constexpr int tiles = EPI == EPI_BIAS_SILU ? 3 : (EPI == EPI_LOSS || EPI == EPI_DSILU) ? 2
+                                                          : EPI == EPI_DSILU_L1 ? 1 : 0;
+    static constexpr int stages = EPI == EPI_BIAS_SILU ? 2 : (tiles ? 3 : 4);
+    static constexpr bool bias = EPI == EPI_BIAS_SILU || EPI == EPI_BIAS_F32 || EPI == EPI_LOSS ||
+                                 EPI == EPI_DSILU_L1;
+    static constexpr int cst = EPI == EPI_DSILU_L1 ? 4 * 256 : (bias ? 256 : 4);
+};
+constexpr uint32_t STAGE_TILE_BYTES = 32 * 64;   // 32 rows x 32 BF16
+constexpr uint32_t XS_BYTES = 32 * 3 * 4;        // a warp's 32 input rows (EPI_DSILU_L1)
+
+template <int EPI>
+__host__ __device__ constexpr size_t gemm_smem_bytes(int N)
+{
+    return 1024 + (size_t)EpiCfg<EPI>::stages * ((size_t)TILE_M * 128 + (size_t)N * 128) +
+           (size_t)EPI_WARPS * (EpiCfg<EPI>::tiles * STAGE_TILE_BYTES + (EPI == EPI_DSILU_L1 ? XS_BYTES : 0));
+}
 
 struct GemmArgs {
     int M, N, K;                    // M % 128 == 0, N % 32 == 0 && 32 <= N <= 256, K % 64 == 0
@@ -93,20 +114,58 @@ __device__ __forceinline__ float dsilu(float z)
     return s * (1.0f + z * (1.0f - s));
 }
 
-// Column sums over the warp's 32 rows of g[32] (one row per lane), added to
-// dst[0..31]; with xs (the rows' inputs), also sum g x_k added to gw[c*3 + k].
-__device__ __forceinline__ void warp_col_sums(float* red, const float* g, int lane, float* dst,
-                                              const float* xs, float* gw)
+// Byte offset of 16-byte piece j (0..3) of row r in a 32-row x 64-byte tile
+// with the 64-byte swizzle of the TMA stores (piece index XOR bits 7-8 of the
+// offset; the tile is 2 KB aligned).  Sixteen-byte stores of 32 rows by 32
+// lanes then touch every bank group equally often (no conflicts).
+__device__ __forceinline__ uint32_t sw64(uint32_t r, uint32_t j)
+{
+    return r * 64u + ((j ^ ((r >> 1) & 3u)) << 4);
+}
+
+// This lane's row of 32 BF16 (h, 16-byte aligned) into a row-major staging tile.
+__device__ __forceinline__ void stage_row(uint8_t* tile, int lane, const bf16* h)
 {
 #pragma unroll
-    for (int i = 0; i < 32; ++i) red[lane * RED_STRIDE + i] = g[i];
+    for (int j = 0; j < 4; ++j)
+        *reinterpret_cast<uint4*>(tile + sw64((uint32_t)lane, (uint32_t)j)) = reinterpret_cast<const uint4*>(h)[j];
+}
+
+// This lane's row of 32 BF16 as column `lane` of a transposed staging tile
+// (tile row c = column c of the chunk); each store writes one tile row of 64
+// bytes across the warp.
+__device__ __forceinline__ void stage_col(uint8_t* tile, int lane, const bf16* h)
+{
+    const uint32_t j = (uint32_t)lane >> 3, e = 2u * ((uint32_t)lane & 7u);
+#pragma unroll
+    for (int c = 0; c < 32; ++c) *reinterpret_cast<bf16*>(tile + sw64((uint32_t)c, j) + e) = h[c];
+}
+
+// Makes this lane's staging writes visible to the TMA unit and joins the warp;
+// then lane 0 may issue the stores.
+__device__ __forceinline__ void stage_done()
+{
+    umma::fence_async_smem();
     __syncwarp();
+}
+
+// Column sums over the warp's 32 rows, read from the transposed staging tile
+// (lane c sums tile row c, rows in order 0..31), added to dst[0..31]; with xs
+// (the rows' inputs), also sum g x_k added to gw[c*3 + k].
+__device__ __forceinline__ void warp_col_sums(const uint8_t* tt, int lane, float* dst, const float* xs, float* gw)
+{
     float s = 0.0f, s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
-#pragma unroll 8
-    for (int r = 0; r < 32; ++r) {
-        const float v = red[r * RED_STRIDE + lane];
-        s += v;
-        if (xs) { s0 += v * xs[r * 3]; s1 += v * xs[r * 3 + 1]; s2 += v * xs[r * 3 + 2]; }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint4 q = *reinterpret_cast<const uint4*>(tt + sw64((uint32_t)lane, (uint32_t)j));
+        const bf16* g8 = reinterpret_cast<const bf16*>(&q);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int r = 8 * j + e;
+            const float v = __bfloat162float(g8[e]);
+            s += v;
+            if (xs) { s0 += v * xs[r * 3]; s1 += v * xs[r * 3 + 1]; s2 += v * xs[r * 3 + 2]; }
+        }
     }
     atomicAdd(dst + lane, s);
     if (xs) {
@@ -114,72 +173,105 @@ __device__ __forceinline__ void warp_col_sums(float* red, const float* g, int la
         atomicAdd(gw + lane * 3 + 1, s1);
         atomicAdd(gw + lane * 3 + 2, s2);
     }
-    __syncwarp();
 }
 
-__device__ __forceinline__ void store_row_bf16(bf16* dst, const bf16* h)
+// Eight consecutive per-column constants from shared memory (all lanes read
+// the same address: a broadcast).
+__device__ __forceinline__ void cst8(const float* c, float* o)
 {
-    uint4* d = reinterpret_cast<uint4*>(dst);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) d[i] = reinterpret_cast<const uint4*>(h)[i];
+    const float4 p = reinterpret_cast<const float4*>(c)[0], q = reinterpret_cast<const float4*>(c)[1];
+    o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = p.w; o[4] = q.x; o[5] = q.y; o[6] = q.z; o[7] = q.w;
 }
 
-// Epilogue of one 128 x N tile: the warp owns rows row0 + 32 (w % 4) + lane and
-// the 32-column chunks c0 = 32 (half + 2 k).
+// TMA output maps of a GEMM: the row-major output (out_h), its transpose
+// (out_ht) and the pre-activations (out_z), boxes of 32 x 32 BF16 with the
+// 64-byte swizzle; maps of absent outputs are unused copies.
+struct OutMaps {
+    CUtensorMap h, ht, z;
+};
+
+// Epilogue of one 128 x N tile: the warp owns rows row0 + lane (row0 = tile
+// row + 32 (w % 4)) and the 32-column chunks c0 = 32 (half + 4 k).  cst holds
+// the bias (and for EPI_DSILU_L1 the columns of W1 at cst + 256 (1 + k)) in
+// shared memory; stg is the warp's staging area (EpiCfg::tiles tiles of 2 KB,
+// then for EPI_DSILU_L1 its rows' inputs).  BF16 outputs leave through TMA
+// stores issued by lane 0; the staging tiles are rewritten only after the
+// previous chunk's stores have read them.
 template <int EPI>
-__device__ __forceinline__ void epilogue(const GemmArgs& G, uint32_t tbase, int row, float* red, int lane,
-                                         int half)
+__device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, uint32_t tbase, int row0,
+                                         int lane, int half, const float* cst, uint8_t* stg, bool& pending)
 {
     const int N = G.N;
+    const int row = row0 + lane;
     float sq = 0.0f;
-    float* xs = red + 32 * RED_STRIDE;
+    float* xs = reinterpret_cast<float*>(stg + EpiCfg<EPI>::tiles * STAGE_TILE_BYTES);
     float x0 = 0.f, x1 = 0.f, x2 = 0.f;
     if (EPI == EPI_DSILU_L1) {
         x0 = G.x[(int64_t)row * 3]; x1 = G.x[(int64_t)row * 3 + 1]; x2 = G.x[(int64_t)row * 3 + 2];
         xs[lane * 3] = x0; xs[lane * 3 + 1] = x1; xs[lane * 3 + 2] = x2;
-        __syncwarp();
     }
     for (int c0 = 32 * half; c0 < N; c0 += 32 * (EPI_WARPS / 4)) {
+        if (EpiCfg<EPI>::tiles) {
+            // the previous chunk's TMA stores have read the staging tiles
+            if (pending && lane == 0) umma::bulk_wait_read0();
+            pending = false;
+            __syncwarp();
+        }
         float v[32];
         umma::tmem_ld32(tbase + (uint32_t)c0, v);
         if (EPI == EPI_F32 || EPI == EPI_BIAS_F32 || EPI == EPI_PARTIAL) {
             float* o = G.out_f + (EPI == EPI_PARTIAL ? (int64_t)blockIdx.y * G.M * G.ldf : 0) +
                        (int64_t)row * G.ldf + c0;
 #pragma unroll
-            for (int i = 0; i < 32; i += 4) {
-                float4 q;
-                q.x = v[i] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i] : 0.0f);
-                q.y = v[i + 1] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i + 1] : 0.0f);
-                q.z = v[i + 2] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i + 2] : 0.0f);
-                q.w = v[i + 3] + (EPI == EPI_BIAS_F32 ? G.bias[c0 + i + 3] : 0.0f);
-                *reinterpret_cast<float4*>(o + i) = q;
+            for (int g = 0; g < 4; ++g) {
+                float b[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (EPI == EPI_BIAS_F32) cst8(cst + c0 + 8 * g, b);
+                float4 q0, q1;
+                q0.x = v[8 * g] + b[0]; q0.y = v[8 * g + 1] + b[1]; q0.z = v[8 * g + 2] + b[2]; q0.w = v[8 * g + 3] + b[3];
+                q1.x = v[8 * g + 4] + b[4]; q1.y = v[8 * g + 5] + b[5]; q1.z = v[8 * g + 6] + b[6]; q1.w = v[8 * g + 7] + b[7];
+                *reinterpret_cast<float4*>(o + 8 * g) = q0;
+                *reinterpret_cast<float4*>(o + 8 * g + 4) = q1;
             }
         } else if (EPI == EPI_BIAS_SILU) {
             __align__(16) bf16 h[32];
             __align__(16) bf16 zz[32];
 #pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                const float z = v[i] + G.bias[c0 + i];
-                zz[i] = __float2bfloat16_rn(z);
-                h[i] = __float2bfloat16_rn(silu(z));
-                if (G.out_ht) G.out_ht[(int64_t)(c0 + i) * G.ldht + row] = h[i];
+            for (int g = 0; g < 4; ++g) {
+                float b[8];
+                cst8(cst + c0 + 8 * g, b);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float z = v[8 * g + q] + b[q];
+                    zz[8 * g + q] = __float2bfloat16_rn(z);
+                    h[8 * g + q] = __float2bfloat16_rn(silu(z));
+                }
             }
-            store_row_bf16(G.out_h + (int64_t)row * G.ldh + c0, h);
-            if (G.out_z) store_row_bf16(G.out_z + (int64_t)row * G.ldh + c0, zz);
+            stage_row(stg, lane, h);
+            if (G.out_ht) stage_col(stg + STAGE_TILE_BYTES, lane, h);
+            if (G.out_z) stage_row(stg + 2 * STAGE_TILE_BYTES, lane, zz);
+            stage_done();
+            if (lane == 0) {
+                umma::tma_store_2d(&om.h, c0, row0, stg);
+                if (G.out_ht) umma::tma_store_2d(&om.ht, row0, c0, stg + STAGE_TILE_BYTES);
+                if (G.out_z) umma::tma_store_2d(&om.z, c0, row0, stg + 2 * STAGE_TILE_BYTES);
+                umma::bulk_commit();
+            }
+            pending = true;
         } else {   // EPI_LOSS, EPI_DSILU, EPI_DSILU_L1: a BF16 gradient and its column sums
             __align__(16) bf16 h[32];
-            float gf[32];
             if (EPI == EPI_LOSS) {
                 const float4* t4 = reinterpret_cast<const float4*>(G.target + (int64_t)row * N + c0);
 #pragma unroll
-                for (int i = 0; i < 32; i += 4) {
-                    const float4 t = t4[i / 4];
-                    const float tt[4] = {t.x, t.y, t.z, t.w};
+                for (int g = 0; g < 4; ++g) {
+                    float b[8];
+                    cst8(cst + c0 + 8 * g, b);
+                    const float4 ta = t4[2 * g], tb = t4[2 * g + 1];
+                    const float tt[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float d = (v[i + q] + G.bias[c0 + i + q]) - tt[q];
+                    for (int q = 0; q < 8; ++q) {
+                        const float d = (v[8 * g + q] + b[q]) - tt[q];
                         sq += d * d;
-                        h[i + q] = __float2bfloat16_rn(2.0f * d * G.scale);
+                        h[8 * g + q] = __float2bfloat16_rn(2.0f * d * G.scale);
                     }
                 }
             } else if (EPI == EPI_DSILU) {
@@ -191,22 +283,38 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, uint32_t tbase, int 
                 for (int i = 0; i < 32; ++i) h[i] = __float2bfloat16_rn(v[i] * dsilu(__bfloat162float(zp[i])));
             } else {
 #pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const int c = c0 + i;
-                    // the forward's pre-activation, same operations in the same order
-                    const float z = G.bias[c] + x0 * G.w1[c * 3] + x1 * G.w1[c * 3 + 1] + x2 * G.w1[c * 3 + 2];
-                    const float zq = __bfloat162float(__float2bfloat16_rn(z));
-                    h[i] = __float2bfloat16_rn(v[i] * dsilu(zq));
+                for (int g = 0; g < 4; ++g) {
+                    float b[8], w0[8], w1[8], w2[8];
+                    cst8(cst + c0 + 8 * g, b);
+                    cst8(cst + 256 + c0 + 8 * g, w0);
+                    cst8(cst + 512 + c0 + 8 * g, w1);
+                    cst8(cst + 768 + c0 + 8 * g, w2);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        // the forward's pre-activation, same operations in the same order
+                        const float z = b[q] + x0 * w0[q] + x1 * w1[q] + x2 * w2[q];
+                        const float zq = __bfloat162float(__float2bfloat16_rn(z));
+                        h[8 * g + q] = __float2bfloat16_rn(v[8 * g + q] * dsilu(zq));
+                    }
                 }
             }
-#pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                gf[i] = __bfloat162float(h[i]);
-                if (EPI != EPI_DSILU_L1 && G.out_ht) G.out_ht[(int64_t)(c0 + i) * G.ldht + row] = h[i];
+            // the transposed tile serves the column sums (and out_ht); EPI_DSILU_L1 writes no BF16 output
+            uint8_t* tt = stg + (EPI == EPI_DSILU_L1 ? 0u : STAGE_TILE_BYTES);
+            if (EPI != EPI_DSILU_L1) stage_row(stg, lane, h);
+            stage_col(tt, lane, h);
+            stage_done();
+            if (EPI != EPI_DSILU_L1) {
+                if (lane == 0) {
+                    if (G.out_h) umma::tma_store_2d(&om.h, c0, row0, stg);
+                    if (G.out_ht) umma::tma_store_2d(&om.ht, row0, c0, tt);
+                    umma::bulk_commit();
+                }
+                pending = true;
             }
-            if (EPI != EPI_DSILU_L1 && G.out_h) store_row_bf16(G.out_h + (int64_t)row * G.ldh + c0, h);
-            warp_col_sums(red, gf, lane, G.colsum + c0, EPI == EPI_DSILU_L1 ? xs : nullptr,
+            warp_col_sums(tt, lane, G.colsum + c0, EPI == EPI_DSILU_L1 ? xs : nullptr,
                           EPI == EPI_DSILU_L1 ? G.gw1 + (int64_t)c0 * 3 : nullptr);
+            // the sums have read the tile before the next chunk may rewrite it
+            __syncwarp();
         }
     }
     if (EPI == EPI_LOSS) {
@@ -228,16 +336,20 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, uint32_t tbase, int 
 template <int EPI>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                const __grid_constant__ GemmArgs G)
+                const __grid_constant__ OutMaps om, const __grid_constant__ GemmArgs G)
 {
+    constexpr int STAGES = EpiCfg<EPI>::stages;
     extern __shared__ uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    // 1024-byte aligned in the shared window (the swizzle atom); offset from
+    // smem_raw so that the compiler still sees shared-memory accesses
+    uint8_t* smem = smem_raw + ((1024u - (umma::smem_u32(smem_raw) & 1023u)) & 1023u);
     const int N = G.N;
     const uint32_t a_bytes = TILE_M * 128, stage_bytes = a_bytes + (uint32_t)N * 128;
-    float* red_all = reinterpret_cast<float*>(smem + STAGES * stage_bytes);
+    uint8_t* stg_all = smem + STAGES * stage_bytes;   // 1024-byte aligned (stage_bytes is)
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
+    __shared__ __align__(16) float s_cst[EpiCfg<EPI>::cst];
 
     const int split = blockIdx.y;
     const int k_begin = split * G.k_split;
@@ -254,7 +366,19 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         abort_flag = 0;
     }
     if (warp == MMA_WARP) umma::tmem_alloc(&tmem_slot, TMEM_COLS);
-    if (warp == PRODUCER_WARP && lane == 0) { umma::prefetch_tmap(&tmA); umma::prefetch_tmap(&tmB); }
+    if (warp == PRODUCER_WARP && lane == 0) {
+        umma::prefetch_tmap(&tmA);
+        umma::prefetch_tmap(&tmB);
+        if (EpiCfg<EPI>::tiles > 0 && EPI != EPI_DSILU_L1) {
+            umma::prefetch_tmap(&om.h);
+            umma::prefetch_tmap(&om.ht);
+            if (EPI == EPI_BIAS_SILU) umma::prefetch_tmap(&om.z);
+        }
+    }
+    if (EpiCfg<EPI>::bias)
+        for (int i = threadIdx.x; i < N; i += blockDim.x) s_cst[i] = G.bias[i];
+    if (EPI == EPI_DSILU_L1)
+        for (int i = threadIdx.x; i < 3 * N; i += blockDim.x) s_cst[256 * (1 + i % 3) + i / 3] = G.w1[i];
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
@@ -314,7 +438,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             if (it > 0) umma::mbar_wait(&empty[(it - 1) % STAGES], ((it - 1) / STAGES) & 1u, WAIT_BUDGET);
         }
     } else {
-        float* red = red_all + warp * (32 * RED_STRIDE + 32 * 3);
+        uint8_t* stg = stg_all + (size_t)warp * (EpiCfg<EPI>::tiles * STAGE_TILE_BYTES +
+                                                (EPI == EPI_DSILU_L1 ? XS_BYTES : 0u));
+        bool pending = false;   // TMA stores of this warp not yet known to have read its tiles
         uint32_t j = 0;
         for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++j) {
             const uint32_t a = j & 1u, u = j >> 1;
@@ -325,12 +451,15 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             }
             umma::fence_after_sync();
             const int quad = warp & 3;
-            const int row = tile * TILE_M + 32 * quad + lane;
-            epilogue<EPI>(G, tmem + a * 256u + ((uint32_t)(32 * quad) << 16), row, red, lane, warp >> 2);
+            epilogue<EPI>(G, om, tmem + a * 256u + ((uint32_t)(32 * quad) << 16), tile * TILE_M + 32 * quad,
+                          lane, warp >> 2, s_cst, stg, pending);
             umma::fence_before_sync();
             __syncwarp();
             if (lane == 0) umma::mbar_arrive(&acc_empty[a]);
         }
+        // the staging tiles stay valid until the TMA stores are complete
+        if (EpiCfg<EPI>::tiles && lane == 0) umma::bulk_wait0();
+        __syncwarp();
     }
     __syncthreads();
     if (warp == MMA_WARP) {
@@ -370,6 +499,21 @@ bool make_map(CUtensorMap* m, const bf16* base, int64_t rows, int64_t K, int64_t
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Store map of a rows x cols BF16 matrix with row stride ld (elements): boxes
+// of 32 x 32 with the 64-byte swizzle of the epilogue's staging tiles.
+bool make_store_map(CUtensorMap* m, const bf16* base, int64_t rows, int64_t cols, int64_t ld)
+{
+    if (!encoder() || !base || ((uintptr_t)base & 15) || (ld * 2) % 16 || cols % 32 || rows % 32 || ld < cols)
+        return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+    const cuuint32_t box[2] = {32, 32};
+    const cuuint32_t estr[2] = {1, 1};
+    return g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                    CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // A [M][K] (row stride lda), B [N][K] (row stride ldb).
 template <int EPI>
 int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int grid_x,
@@ -381,6 +525,15 @@ int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, in
         return CL_ERR_ARG;
     CUtensorMap ta, tb;
     if (!make_map(&ta, A, g.M, g.K, lda, TILE_M) || !make_map(&tb, B, g.N, g.K, ldb, g.N)) return CL_ERR_ARG;
+    // output maps of the staged epilogues (unused ones are copies of ta)
+    OutMaps om;
+    om.h = om.ht = om.z = ta;
+    if (EpiCfg<EPI>::tiles > 0 && EPI != EPI_DSILU_L1) {
+        if (!g.out_h || !make_store_map(&om.h, g.out_h, g.M, g.N, g.ldh)) return CL_ERR_ARG;
+        if (g.out_ht && !make_store_map(&om.ht, g.out_ht, g.N, g.M, g.ldht)) return CL_ERR_ARG;
+        if (EPI == EPI_BIAS_SILU && g.out_z && !make_store_map(&om.z, g.out_z, g.M, g.N, g.ldh)) return CL_ERR_ARG;
+        if ((EPI == EPI_LOSS || EPI == EPI_DSILU) && !g.out_ht) return CL_ERR_ARG;
+    }
     // the shared-memory opt-in is a per-device attribute of the kernel: set it
     // once for every device this process launches on
     static std::atomic<uint64_t> attr_devices{0};
@@ -389,15 +542,15 @@ int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, in
     const uint64_t bit = 1ull << (dev & 63);
     if (!(attr_devices.load() & bit)) {
         if (cudaFuncSetAttribute(gemm_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)gemm_smem_bytes(256)) != cudaSuccess)
+                                 (int)gemm_smem_bytes<EPI>(256)) != cudaSuccess)
             return CL_ERR_CUDA;
         attr_devices.fetch_or(bit);
     }
     const int tiles = g.M / TILE_M;
     dim3 grid((unsigned)(grid_x < tiles ? grid_x : tiles), (unsigned)splits);
     // at least 116 KB so that one CTA holds an SM: each allocates all 512 TMEM columns
-    const size_t smem = gemm_smem_bytes(g.N) > 116 * 1024 ? gemm_smem_bytes(g.N) : 116 * 1024;
-    gemm_kernel<EPI><<<grid, GEMM_THREADS, smem, st>>>(ta, tb, g);
+    const size_t smem = gemm_smem_bytes<EPI>(g.N) > 116 * 1024 ? gemm_smem_bytes<EPI>(g.N) : 116 * 1024;
+    gemm_kernel<EPI><<<grid, GEMM_THREADS, smem, st>>>(ta, tb, om, g);
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
 }
 

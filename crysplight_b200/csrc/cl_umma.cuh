@@ -153,6 +153,31 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int32_t
         : "memory");
 }
 
+// 2-D tiled TMA store of a shared-memory box to element coordinates (x =
+// inner, y = row); completion tracked by bulk groups of the issuing thread.
+__device__ __forceinline__ void tma_store_2d(const void* tmap, int32_t x, int32_t y, const void* src)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+                 :: "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(src)) : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit()
+{
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// Wait until every committed bulk store of this thread has read its source.
+__device__ __forceinline__ void bulk_wait_read0()
+{
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Wait until every committed bulk store of this thread is complete.
+__device__ __forceinline__ void bulk_wait0()
+{
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 __device__ __forceinline__ void prefetch_tmap(const void* tmap)
 {
     asm volatile("prefetch.tensormap [%0];" :: "l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
