@@ -76,6 +76,9 @@ struct EpiCfg {
     static constexpr bool bias = EPI == EPI_BIAS_SILU || EPI == EPI_BIAS_F32 || EPI == EPI_LOSS ||
                                  EPI == EPI_DSILU_L1;
     static constexpr int cst = EPI == EPI_DSILU_L1 ? 4 * 256 : (bias ? 256 : 4);
+    // CTA accumulators of the column sums (bias gradient; for EPI_DSILU_L1
+    // also the layer-1 weight gradient by input component), flushed once
+    static constexpr int acc = EPI == EPI_DSILU_L1 ? 4 * 256 : (tiles >= 2 && EPI != EPI_BIAS_SILU) ? 256 : 4;
 };
 constexpr uint32_t STAGE_TILE_BYTES = 32 * 64;   // 32 rows x 32 BF16
 constexpr uint32_t XS_BYTES = 32 * 3 * 4;        // a warp's 32 input rows (EPI_DSILU_L1)
@@ -96,7 +99,8 @@ struct GemmArgs {
     bf16* out_ht; int64_t ldht;     // [N][M]
     bf16* out_z;                    // [M][N], ld = ldh
     const bf16* zprev;              // [M][N], ld = ldh
-    const float* target;            // EPI_LOSS: [M][N] FP32
+    const float* target;            // EPI_LOSS: FP32 rows of N targets
+    const int32_t* trow;            // EPI_LOSS: target row of each batch row (nullptr: the same row)
     float scale;
     float* loss;
     float* colsum;                  // [N]
@@ -149,9 +153,18 @@ __device__ __forceinline__ void stage_done()
     __syncwarp();
 }
 
+// Eight consecutive per-column constants (or row inputs) from shared memory (all lanes read
+// the same address: a broadcast).
+__device__ __forceinline__ void cst8(const float* c, float* o)
+{
+    const float4 p = reinterpret_cast<const float4*>(c)[0], q = reinterpret_cast<const float4*>(c)[1];
+    o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = p.w; o[4] = q.x; o[5] = q.y; o[6] = q.z; o[7] = q.w;
+}
+
 // Column sums over the warp's 32 rows, read from the transposed staging tile
 // (lane c sums tile row c, rows in order 0..31), added to dst[0..31]; with xs
-// (the rows' inputs), also sum g x_k added to gw[c*3 + k].
+// (the rows' inputs by component, xs[32 k + r]), also sum g x_k added to
+// gw[256 k + c].  dst and gw are the CTA's shared-memory accumulators.
 __device__ __forceinline__ void warp_col_sums(const uint8_t* tt, int lane, float* dst, const float* xs, float* gw)
 {
     float s = 0.0f, s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
@@ -159,28 +172,21 @@ __device__ __forceinline__ void warp_col_sums(const uint8_t* tt, int lane, float
     for (int j = 0; j < 4; ++j) {
         const uint4 q = *reinterpret_cast<const uint4*>(tt + sw64((uint32_t)lane, (uint32_t)j));
         const bf16* g8 = reinterpret_cast<const bf16*>(&q);
+        float xa[8], xb[8], xc[8];
+        if (xs) { cst8(xs + 8 * j, xa); cst8(xs + 32 + 8 * j, xb); cst8(xs + 64 + 8 * j, xc); }
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-            const int r = 8 * j + e;
             const float v = __bfloat162float(g8[e]);
             s += v;
-            if (xs) { s0 += v * xs[r * 3]; s1 += v * xs[r * 3 + 1]; s2 += v * xs[r * 3 + 2]; }
+            if (xs) { s0 += v * xa[e]; s1 += v * xb[e]; s2 += v * xc[e]; }
         }
     }
     atomicAdd(dst + lane, s);
     if (xs) {
-        atomicAdd(gw + lane * 3, s0);
-        atomicAdd(gw + lane * 3 + 1, s1);
-        atomicAdd(gw + lane * 3 + 2, s2);
+        atomicAdd(gw + lane, s0);
+        atomicAdd(gw + 256 + lane, s1);
+        atomicAdd(gw + 512 + lane, s2);
     }
-}
-
-// Eight consecutive per-column constants from shared memory (all lanes read
-// the same address: a broadcast).
-__device__ __forceinline__ void cst8(const float* c, float* o)
-{
-    const float4 p = reinterpret_cast<const float4*>(c)[0], q = reinterpret_cast<const float4*>(c)[1];
-    o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = p.w; o[4] = q.x; o[5] = q.y; o[6] = q.z; o[7] = q.w;
 }
 
 // TMA output maps of a GEMM: the row-major output (out_h), its transpose
@@ -199,7 +205,8 @@ struct OutMaps {
 // previous chunk's stores have read them.
 template <int EPI>
 __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, uint32_t tbase, int row0,
-                                         int lane, int half, const float* cst, uint8_t* stg, bool& pending)
+                                         int lane, int half, const float* cst, uint8_t* stg, bool& pending,
+                                         float* acc)
 {
     const int N = G.N;
     const int row = row0 + lane;
@@ -208,7 +215,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
     float x0 = 0.f, x1 = 0.f, x2 = 0.f;
     if (EPI == EPI_DSILU_L1) {
         x0 = G.x[(int64_t)row * 3]; x1 = G.x[(int64_t)row * 3 + 1]; x2 = G.x[(int64_t)row * 3 + 2];
-        xs[lane * 3] = x0; xs[lane * 3 + 1] = x1; xs[lane * 3 + 2] = x2;
+        xs[lane] = x0; xs[32 + lane] = x1; xs[64 + lane] = x2;
     }
     for (int c0 = 32 * half; c0 < N; c0 += 32 * (EPI_WARPS / 4)) {
         if (EpiCfg<EPI>::tiles) {
@@ -260,7 +267,8 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
         } else {   // EPI_LOSS, EPI_DSILU, EPI_DSILU_L1: a BF16 gradient and its column sums
             __align__(16) bf16 h[32];
             if (EPI == EPI_LOSS) {
-                const float4* t4 = reinterpret_cast<const float4*>(G.target + (int64_t)row * N + c0);
+                const int64_t tr = G.trow ? (int64_t)G.trow[row] : (int64_t)row;
+                const float4* t4 = reinterpret_cast<const float4*>(G.target + tr * N + c0);
 #pragma unroll
                 for (int g = 0; g < 4; ++g) {
                     float b[8];
@@ -311,8 +319,8 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
                 }
                 pending = true;
             }
-            warp_col_sums(tt, lane, G.colsum + c0, EPI == EPI_DSILU_L1 ? xs : nullptr,
-                          EPI == EPI_DSILU_L1 ? G.gw1 + (int64_t)c0 * 3 : nullptr);
+            warp_col_sums(tt, lane, acc + c0, EPI == EPI_DSILU_L1 ? xs : nullptr,
+                          EPI == EPI_DSILU_L1 ? acc + 256 + c0 : nullptr);
             // the sums have read the tile before the next chunk may rewrite it
             __syncwarp();
         }
@@ -350,6 +358,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     __shared__ __align__(16) float s_cst[EpiCfg<EPI>::cst];
+    __shared__ float s_acc[EpiCfg<EPI>::acc];
 
     const int split = blockIdx.y;
     const int k_begin = split * G.k_split;
@@ -379,6 +388,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         for (int i = threadIdx.x; i < N; i += blockDim.x) s_cst[i] = G.bias[i];
     if (EPI == EPI_DSILU_L1)
         for (int i = threadIdx.x; i < 3 * N; i += blockDim.x) s_cst[256 * (1 + i % 3) + i / 3] = G.w1[i];
+    for (int i = threadIdx.x; i < EpiCfg<EPI>::acc; i += blockDim.x) s_acc[i] = 0.0f;
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
@@ -452,7 +462,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             umma::fence_after_sync();
             const int quad = warp & 3;
             epilogue<EPI>(G, om, tmem + a * 256u + ((uint32_t)(32 * quad) << 16), tile * TILE_M + 32 * quad,
-                          lane, warp >> 2, s_cst, stg, pending);
+                          lane, warp >> 2, s_cst, stg, pending, s_acc);
             umma::fence_before_sync();
             __syncwarp();
             if (lane == 0) umma::mbar_arrive(&acc_empty[a]);
@@ -465,6 +475,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     if (warp == MMA_WARP) {
         umma::fence_after_sync();
         umma::tmem_dealloc(tmem, TMEM_COLS);
+    }
+    // the CTA's column sums, one global atomic per column
+    if (EPI == EPI_LOSS || EPI == EPI_DSILU || EPI == EPI_DSILU_L1) {
+        for (int i = threadIdx.x; i < N; i += blockDim.x) atomicAdd(G.colsum + i, s_acc[i]);
+        if (EPI == EPI_DSILU_L1)
+            for (int i = threadIdx.x; i < 3 * N; i += blockDim.x)
+                atomicAdd(G.gw1 + i, s_acc[256 + 256 * (i % 3) + i / 3]);
     }
 }
 
@@ -576,19 +593,19 @@ __device__ __forceinline__ uint32_t hash32(uint32_t a, uint32_t b, uint32_t c)
     return c0;
 }
 
-// Random minibatch (with replacement) from the training set.
-__global__ void __launch_bounds__(256) gather_batch(const float* __restrict__ X, const float* __restrict__ T,
-                                                    int64_t n_all, int B, uint32_t seed, uint32_t step,
-                                                    float* Xb, float* Tb)
+// Random minibatch (with replacement) from the training set: the inputs are
+// copied (Xb), the targets are read in place by the loss epilogue through the
+// row indices (rows).
+__global__ void __launch_bounds__(256) gather_batch(const float* __restrict__ X, int64_t n_all, int B,
+                                                    uint32_t seed, uint32_t step, float* Xb, int32_t* rows)
 {
-    // one warp per row: the target row (192 floats) as 48 float4
-    const int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    const int b = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     if (b >= B) return;
     const int64_t i = (int64_t)(hash32((uint32_t)b, step, seed) % (uint32_t)n_all);
-    if (lane < D_IN) Xb[(int64_t)b * D_IN + lane] = X[i * D_IN + lane];
-    const float4* src = reinterpret_cast<const float4*>(T + i * D_OUT);
-    float4* dst = reinterpret_cast<float4*>(Tb + (int64_t)b * D_OUT);
-    for (int j = lane; j < D_OUT / 4; j += 32) dst[j] = src[j];
+    rows[b] = (int32_t)i;
+    Xb[(int64_t)b * D_IN] = X[i * D_IN];
+    Xb[(int64_t)b * D_IN + 1] = X[i * D_IN + 1];
+    Xb[(int64_t)b * D_IN + 2] = X[i * D_IN + 2];
 }
 
 // Layer 1 (K = 3) on the CUDA cores: h = silu(x W1^T + b1) for 64 rows per
@@ -621,15 +638,33 @@ __global__ void __launch_bounds__(256) layer1_fwd(const float* __restrict__ X, c
     }
 }
 
-// grad_Wt[o][i] = sum_s P[s][i][o]   (P: split-K partials of dW = H^T dZ, [IN][OUT])
-__global__ void reduce_wgrad(const float* __restrict__ P, int S, int IN, int OUT, float* gWt)
+// grad_Wt[o][i] = sum_s P[s][i][o]   (P: split-K partials of dW = H^T dZ, [IN][OUT]),
+// summed in split order.  A block takes 64 consecutive entries of [IN][OUT]:
+// all 256 threads stage 64 splits of them in shared memory (coalesced rows of
+// 256 bytes, 16 loads in flight per thread), then 64 threads sum a column each.
+constexpr int RW_COLS = 64, RW_SPLITS = 64;
+__global__ void __launch_bounds__(256) reduce_wgrad(const float* __restrict__ P, int S, int IN, int OUT, float* gWt)
 {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= IN * OUT) return;
-    const int i = idx / OUT, o = idx % OUT;
+    __shared__ float tile[RW_SPLITS][RW_COLS + 1];
+    const int64_t n = (int64_t)IN * OUT;
+    const int64_t e0 = (int64_t)blockIdx.x * RW_COLS;
+    const int c = threadIdx.x % RW_COLS, r = threadIdx.x / RW_COLS;
     float acc = 0.0f;
-    for (int s = 0; s < S; ++s) acc += P[((int64_t)s * IN + i) * OUT + o];
-    gWt[(int64_t)o * IN + i] = acc;
+    for (int s0 = 0; s0 < S; s0 += RW_SPLITS) {
+        const int ns = S - s0 < RW_SPLITS ? S - s0 : RW_SPLITS;
+        __syncthreads();
+#pragma unroll 16
+        for (int sr = r; sr < ns; sr += 256 / RW_COLS)
+            tile[sr][c] = e0 + c < n ? __ldg(P + (int64_t)(s0 + sr) * n + e0 + c) : 0.0f;
+        __syncthreads();
+        if (threadIdx.x < RW_COLS)
+            for (int sr = 0; sr < ns; ++sr) acc += tile[sr][threadIdx.x];
+    }
+    const int64_t e = e0 + threadIdx.x;
+    if (threadIdx.x < RW_COLS && e < n) {
+        const int i = (int)(e / OUT), o = (int)(e % OUT);
+        gWt[(int64_t)o * IN + i] = acc;
+    }
 }
 
 // Adam on an FP32 master tensor; optional BF16 copies of a [OUT][IN] matrix
@@ -703,7 +738,8 @@ struct cl_mlp {
     // BF16 weight copies
     bf16 *w2t = nullptr, *w2 = nullptr, *w3t = nullptr, *w3 = nullptr, *w4t = nullptr, *w4 = nullptr;
     // activations and gradients (max_batch rows)
-    float *xb = nullptr, *tb = nullptr, *o = nullptr;
+    float *xb = nullptr, *o = nullptr;
+    int32_t* brow = nullptr;        // training-set row of each minibatch row
     bf16 *h1 = nullptr, *h1t = nullptr, *h2 = nullptr, *h2t = nullptr, *z2 = nullptr;
     bf16 *h3 = nullptr, *h3t = nullptr, *z3 = nullptr;
     bf16 *dO = nullptr, *dOt = nullptr, *dz3 = nullptr, *dz3t = nullptr, *dz2 = nullptr, *dz2t = nullptr;
@@ -762,8 +798,9 @@ GemmArgs gemm_args(cl_mlp* m)
 
 // Forward pass over B rows of m->xb (B % 128 == 0).  Training (with_loss):
 // keeps Z, H^T for the backward pass and ends in the loss epilogue, which
-// writes dO, dO^T, the b4 gradient and the loss.  Inference: O into m->o.
-int forward(cl_mlp* m, int B, bool with_loss, cudaStream_t st)
+// reads the targets (rows `trow` of `target`, or its first B rows) and writes
+// dO, dO^T, the b4 gradient and the loss.  Inference: O into m->o.
+int forward(cl_mlp* m, int B, bool with_loss, const float* target, const int32_t* trow, cudaStream_t st)
 {
     const int grid = grid_for(m, B);
     if (with_loss) cudaMemsetAsync(m->g, 0, N_PARAMS * sizeof(float), st);
@@ -784,7 +821,7 @@ int forward(cl_mlp* m, int B, bool with_loss, cudaStream_t st)
         q.out_f = m->o; q.ldf = D_OUT;
         return launch_gemm<EPI_BIAS_F32>(q, m->h3, D_H, m->w4t, D_H, grid, 1, st);
     }
-    q.target = m->tb; q.scale = 1.0f / ((float)B * (float)D_OUT); q.loss = m->loss;
+    q.target = target; q.trow = trow; q.scale = 1.0f / ((float)B * (float)D_OUT); q.loss = m->loss;
     q.out_h = m->dO; q.ldh = D_OUT; q.out_ht = m->dOt; q.ldht = B; q.colsum = m->g + OFF_B4;
     return launch_gemm<EPI_LOSS>(q, m->h3, D_H, m->w4t, D_H, grid, 1, st);
 }
@@ -818,7 +855,7 @@ int backward(cl_mlp* m, int B, cudaStream_t st)
         w.M = D_H; w.N = wg[l].OUT; w.K = B; w.k_split = WGRAD_SPLIT_K;
         w.out_f = m->part; w.ldf = wg[l].OUT;
         if ((rc = launch_gemm<EPI_PARTIAL>(w, wg[l].ht, B, wg[l].dzt, B, D_H / TILE_M, splits, st))) return rc;
-        reduce_wgrad<<<(D_H * wg[l].OUT + 255) / 256, 256, 0, st>>>(m->part, splits, D_H, wg[l].OUT,
+        reduce_wgrad<<<(D_H * wg[l].OUT + RW_COLS - 1) / RW_COLS, 256, 0, st>>>(m->part, splits, D_H, wg[l].OUT,
                                                                     m->g + wg[l].off_w);
     }
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
@@ -870,7 +907,7 @@ int cl_mlp_create(cl_mlp** out, int device, int max_batch)
               dalloc(m, &m->w2t, (size_t)D_H * D_H) && dalloc(m, &m->w2, (size_t)D_H * D_H) &&
               dalloc(m, &m->w3t, (size_t)D_H * D_H) && dalloc(m, &m->w3, (size_t)D_H * D_H) &&
               dalloc(m, &m->w4t, (size_t)D_OUT * D_H) && dalloc(m, &m->w4, (size_t)D_OUT * D_H) &&
-              dalloc(m, &m->xb, B * D_IN) && dalloc(m, &m->tb, B * D_OUT) && dalloc(m, &m->o, B * D_OUT) &&
+              dalloc(m, &m->xb, B * D_IN) && dalloc(m, &m->brow, B) && dalloc(m, &m->o, B * D_OUT) &&
               dalloc(m, &m->h1, B * D_H) && dalloc(m, &m->h1t, B * D_H) &&
               dalloc(m, &m->h2, B * D_H) && dalloc(m, &m->h2t, B * D_H) && dalloc(m, &m->z2, B * D_H) &&
               dalloc(m, &m->h3, B * D_H) && dalloc(m, &m->h3t, B * D_H) && dalloc(m, &m->z3, B * D_H) &&
@@ -957,9 +994,9 @@ int cl_mlp_train(cl_mlp* m, int steps, int batch, float lr, uint32_t seed, uint3
     cudaStream_t st = m->stream;
     cudaMemsetAsync(m->loss, 0, sizeof(float), st);
     for (int s = 0; s < steps; ++s) {
-        gather_batch<<<(batch + 7) / 8, 256, 0, st>>>(m->data_x, m->data_t, m->n_data, batch, seed, step0 + (uint32_t)s,
-                                          m->xb, m->tb);
-        int rc = forward(m, batch, true, st);
+        gather_batch<<<(batch + 255) / 256, 256, 0, st>>>(m->data_x, m->n_data, batch, seed, step0 + (uint32_t)s,
+                                                          m->xb, m->brow);
+        int rc = forward(m, batch, true, m->data_t, m->brow, st);
         if (!rc) rc = backward(m, batch, st);
         if (rc) return mlp_fail(m, rc, "kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
         adam(m, lr, st);
@@ -985,7 +1022,7 @@ int cl_mlp_forward(cl_mlp* m, const float* d_x, float* d_out, int64_t n)
         const int B = ((rows + TILE_M - 1) / TILE_M) * TILE_M;
         cudaMemsetAsync(m->xb, 0, (size_t)B * D_IN * sizeof(float), st);
         cudaMemcpyAsync(m->xb, d_x + r0 * D_IN, (size_t)rows * D_IN * sizeof(float), cudaMemcpyDeviceToDevice, st);
-        int rc = forward(m, B, false, st);
+        int rc = forward(m, B, false, nullptr, nullptr, st);
         if (rc) return mlp_fail(m, rc, "forward launch failed");
         cudaMemcpyAsync(d_out + r0 * D_OUT, m->o, (size_t)rows * D_OUT * sizeof(float), cudaMemcpyDeviceToDevice, st);
     }
@@ -1003,9 +1040,8 @@ int cl_mlp_gradient(cl_mlp* m, const float* d_x, const float* d_t, int B, float*
     cudaSetDevice(m->device);
     cudaStream_t st = m->stream;
     cudaMemcpyAsync(m->xb, d_x, (size_t)B * D_IN * sizeof(float), cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(m->tb, d_t, (size_t)B * D_OUT * sizeof(float), cudaMemcpyDeviceToDevice, st);
     cudaMemsetAsync(m->loss, 0, sizeof(float), st);
-    int rc = forward(m, B, true, st);
+    int rc = forward(m, B, true, d_t, nullptr, st);
     if (!rc) rc = backward(m, B, st);
     if (rc) return mlp_fail(m, rc, "launch failed");
     float loss = 0.0f;
