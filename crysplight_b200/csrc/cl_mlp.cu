@@ -61,6 +61,7 @@ enum Epi : int {
     EPI_PARTIAL = 4,     // out_f[split][m][n] = acc (split-K partial)
     EPI_LOSS = 5,        // o = acc + b, d = o - target: loss += scale d^2, g = bf16(2 scale d) -> out_h, out_ht, colsum
     EPI_DSILU_L1 = 6,    // as EPI_DSILU with zprev recomputed from x, W1, b1; colsum and gw1 += g, g x
+    EPI_WGRAD = 7,       // out_f[n][m] += acc (a K split of a weight gradient, added in place, transposed)
 };
 
 // Per epilogue: the BF16 tiles each epilogue warp stages in shared memory per
@@ -224,9 +225,30 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
             pending = false;
             __syncwarp();
         }
+        // the chunk's global inputs are requested before the accumulator is
+        // read, so that their latency overlaps the tensor-memory load
+        float4 tg[8];
+        uint4 zp4[4];
+        if (EPI == EPI_LOSS) {
+            const int64_t tr = G.trow ? (int64_t)G.trow[row] : (int64_t)row;
+            const float4* t4 = reinterpret_cast<const float4*>(G.target + tr * N + c0);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) tg[i] = t4[i];
+        }
+        if (EPI == EPI_DSILU) {
+            const uint4* z4 = reinterpret_cast<const uint4*>(G.zprev + (int64_t)row * G.ldh + c0);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) zp4[i] = z4[i];
+        }
         float v[32];
         umma::tmem_ld32(tbase + (uint32_t)c0, v);
-        if (EPI == EPI_F32 || EPI == EPI_BIAS_F32 || EPI == EPI_PARTIAL) {
+        if (EPI == EPI_WGRAD) {
+            // column n of the tile is row n of the transposed output: the warp's
+            // 32 rows are 32 consecutive floats there (one coalesced reduction)
+            float* o = G.out_f + (int64_t)c0 * G.ldf + row;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) atomicAdd(o + (int64_t)i * G.ldf, v[i]);
+        } else if (EPI == EPI_F32 || EPI == EPI_BIAS_F32 || EPI == EPI_PARTIAL) {
             float* o = G.out_f + (EPI == EPI_PARTIAL ? (int64_t)blockIdx.y * G.M * G.ldf : 0) +
                        (int64_t)row * G.ldf + c0;
 #pragma unroll
@@ -267,13 +289,11 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
         } else {   // EPI_LOSS, EPI_DSILU, EPI_DSILU_L1: a BF16 gradient and its column sums
             __align__(16) bf16 h[32];
             if (EPI == EPI_LOSS) {
-                const int64_t tr = G.trow ? (int64_t)G.trow[row] : (int64_t)row;
-                const float4* t4 = reinterpret_cast<const float4*>(G.target + tr * N + c0);
 #pragma unroll
                 for (int g = 0; g < 4; ++g) {
                     float b[8];
                     cst8(cst + c0 + 8 * g, b);
-                    const float4 ta = t4[2 * g], tb = t4[2 * g + 1];
+                    const float4 ta = tg[2 * g], tb = tg[2 * g + 1];
                     const float tt[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
@@ -284,9 +304,8 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
                 }
             } else if (EPI == EPI_DSILU) {
                 __align__(16) bf16 zp[32];
-                const uint4* z4 = reinterpret_cast<const uint4*>(G.zprev + (int64_t)row * G.ldh + c0);
 #pragma unroll
-                for (int i = 0; i < 4; ++i) reinterpret_cast<uint4*>(zp)[i] = z4[i];
+                for (int i = 0; i < 4; ++i) reinterpret_cast<uint4*>(zp)[i] = zp4[i];
 #pragma unroll
                 for (int i = 0; i < 32; ++i) h[i] = __float2bfloat16_rn(v[i] * dsilu(__bfloat162float(zp[i])));
             } else {
@@ -638,35 +657,6 @@ __global__ void __launch_bounds__(256) layer1_fwd(const float* __restrict__ X, c
     }
 }
 
-// grad_Wt[o][i] = sum_s P[s][i][o]   (P: split-K partials of dW = H^T dZ, [IN][OUT]),
-// summed in split order.  A block takes 64 consecutive entries of [IN][OUT]:
-// all 256 threads stage 64 splits of them in shared memory (coalesced rows of
-// 256 bytes, 16 loads in flight per thread), then 64 threads sum a column each.
-constexpr int RW_COLS = 64, RW_SPLITS = 64;
-__global__ void __launch_bounds__(256) reduce_wgrad(const float* __restrict__ P, int S, int IN, int OUT, float* gWt)
-{
-    __shared__ float tile[RW_SPLITS][RW_COLS + 1];
-    const int64_t n = (int64_t)IN * OUT;
-    const int64_t e0 = (int64_t)blockIdx.x * RW_COLS;
-    const int c = threadIdx.x % RW_COLS, r = threadIdx.x / RW_COLS;
-    float acc = 0.0f;
-    for (int s0 = 0; s0 < S; s0 += RW_SPLITS) {
-        const int ns = S - s0 < RW_SPLITS ? S - s0 : RW_SPLITS;
-        __syncthreads();
-#pragma unroll 16
-        for (int sr = r; sr < ns; sr += 256 / RW_COLS)
-            tile[sr][c] = e0 + c < n ? __ldg(P + (int64_t)(s0 + sr) * n + e0 + c) : 0.0f;
-        __syncthreads();
-        if (threadIdx.x < RW_COLS)
-            for (int sr = 0; sr < ns; ++sr) acc += tile[sr][threadIdx.x];
-    }
-    const int64_t e = e0 + threadIdx.x;
-    if (threadIdx.x < RW_COLS && e < n) {
-        const int i = (int)(e / OUT), o = (int)(e % OUT);
-        gWt[(int64_t)o * IN + i] = acc;
-    }
-}
-
 // Adam on an FP32 master tensor; optional BF16 copies of a [OUT][IN] matrix
 // in both layouts ([OUT][IN] for the forward B operand, [IN][OUT] for the
 // backward-data B operand).
@@ -743,7 +733,6 @@ struct cl_mlp {
     bf16 *h1 = nullptr, *h1t = nullptr, *h2 = nullptr, *h2t = nullptr, *z2 = nullptr;
     bf16 *h3 = nullptr, *h3t = nullptr, *z3 = nullptr;
     bf16 *dO = nullptr, *dOt = nullptr, *dz3 = nullptr, *dz3t = nullptr, *dz2 = nullptr, *dz2t = nullptr;
-    float* part = nullptr;          // split-K partials
     float* loss = nullptr;          // device accumulator
     unsigned int* derr = nullptr;
     // training set (device pointers owned by the caller)
@@ -846,17 +835,16 @@ int backward(cl_mlp* m, int B, cudaStream_t st)
     l1.bias = m->p + OFF_B1; l1.x = m->xb; l1.w1 = m->p + OFF_W1;
     l1.colsum = m->g + OFF_B1; l1.gw1 = m->g + OFF_W1;
     if ((rc = launch_gemm<EPI_DSILU_L1>(l1, m->dz2, D_H, m->w2, D_H, grid, 1, st))) return rc;
-    // weight gradients dW = H^T dZ (split-K over the batch) -> grad W^T
+    // weight gradients dW = H^T dZ (split-K over the batch), each split added
+    // in place into grad W^T (zeroed by the forward pass)
     const int splits = (B + WGRAD_SPLIT_K - 1) / WGRAD_SPLIT_K;
     struct WG { const bf16* ht; const bf16* dzt; int OUT; int64_t off_w; };
     const WG wg[3] = {{m->h3t, m->dOt, D_OUT, OFF_W4}, {m->h2t, m->dz3t, D_H, OFF_W3}, {m->h1t, m->dz2t, D_H, OFF_W2}};
     for (int l = 0; l < 3; ++l) {
         GemmArgs w = gemm_args(m);
         w.M = D_H; w.N = wg[l].OUT; w.K = B; w.k_split = WGRAD_SPLIT_K;
-        w.out_f = m->part; w.ldf = wg[l].OUT;
-        if ((rc = launch_gemm<EPI_PARTIAL>(w, wg[l].ht, B, wg[l].dzt, B, D_H / TILE_M, splits, st))) return rc;
-        reduce_wgrad<<<(D_H * wg[l].OUT + RW_COLS - 1) / RW_COLS, 256, 0, st>>>(m->part, splits, D_H, wg[l].OUT,
-                                                                    m->g + wg[l].off_w);
+        w.out_f = m->g + wg[l].off_w; w.ldf = D_H;
+        if ((rc = launch_gemm<EPI_WGRAD>(w, wg[l].ht, B, wg[l].dzt, B, D_H / TILE_M, splits, st))) return rc;
     }
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
 }
@@ -901,7 +889,6 @@ int cl_mlp_create(cl_mlp** out, int device, int max_batch)
         return CL_ERR_CUDA;
     }
     const size_t B = (size_t)max_batch;
-    const int splits = (max_batch + WGRAD_SPLIT_K - 1) / WGRAD_SPLIT_K;
     bool ok = dalloc(m, &m->p, N_PARAMS) && dalloc(m, &m->g, N_PARAMS) && dalloc(m, &m->m, N_PARAMS) &&
               dalloc(m, &m->v, N_PARAMS) &&
               dalloc(m, &m->w2t, (size_t)D_H * D_H) && dalloc(m, &m->w2, (size_t)D_H * D_H) &&
@@ -914,7 +901,7 @@ int cl_mlp_create(cl_mlp** out, int device, int max_batch)
               dalloc(m, &m->dO, B * D_OUT) && dalloc(m, &m->dOt, B * D_OUT) &&
               dalloc(m, &m->dz3, B * D_H) && dalloc(m, &m->dz3t, B * D_H) &&
               dalloc(m, &m->dz2, B * D_H) && dalloc(m, &m->dz2t, B * D_H) &&
-              dalloc(m, &m->part, (size_t)splits * D_H * D_H) && dalloc(m, &m->loss, 1) &&
+              dalloc(m, &m->loss, 1) &&
               dalloc(m, &m->derr, 1);
     if (!ok) {
         for (void* q : m->allocs) cudaFree(q);
