@@ -61,7 +61,8 @@ enum Epi : int {
     EPI_PARTIAL = 4,     // out_f[split][m][n] = acc (split-K partial)
     EPI_LOSS = 5,        // o = acc + b, d = o - target: loss += scale d^2, g = bf16(2 scale d) -> out_h, out_ht, colsum
     EPI_DSILU_L1 = 6,    // as EPI_DSILU with zprev recomputed from x, W1, b1; colsum and gw1 += g, g x
-    EPI_WGRAD = 7,       // out_f[n][m] += acc (a K split of a weight gradient, added in place, transposed)
+    EPI_WGRAD = 7,       // out_f[n][m] += acc (a K split of a weight gradient, added in place, transposed);
+                         // A [K][M] and B [K][N] MN-major (the activations and gradients as stored)
 };
 
 // Per epilogue: the BF16 tiles each epilogue warp stages in shared memory per
@@ -366,6 +367,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                 const __grid_constant__ OutMaps om, const __grid_constant__ GemmArgs G)
 {
     constexpr int STAGES = EpiCfg<EPI>::stages;
+    constexpr bool MN = EPI == EPI_WGRAD;   // MN-major operands
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte aligned in the shared window (the swizzle atom); offset from
     // smem_raw so that the compiler still sees shared-memory accesses
@@ -426,8 +428,17 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                     }
                     uint8_t* st = smem + s * stage_bytes;
                     umma::mbar_arrive_expect_tx(&full[s], stage_bytes);
-                    umma::tma_load_2d(st, &tmA, k_begin + c * TILE_K, tile * TILE_M, &full[s]);
-                    umma::tma_load_2d(st + a_bytes, &tmB, k_begin + c * TILE_K, 0, &full[s]);
+                    const int k0 = k_begin + c * TILE_K;
+                    if (MN) {
+                        // boxes of 64 MN-elements x 64 K-rows, 8 KB apart
+                        umma::tma_load_2d(st, &tmA, tile * TILE_M, k0, &full[s]);
+                        umma::tma_load_2d(st + 8192, &tmA, tile * TILE_M + 64, k0, &full[s]);
+                        for (int q = 0; q < N / 64; ++q)
+                            umma::tma_load_2d(st + a_bytes + 8192 * q, &tmB, 64 * q, k0, &full[s]);
+                    } else {
+                        umma::tma_load_2d(st, &tmA, k0, tile * TILE_M, &full[s]);
+                        umma::tma_load_2d(st + a_bytes, &tmB, k0, 0, &full[s]);
+                    }
                 }
             }
             if (!ok) { atomicOr(G.err, 1u); *abort_v = 1; }
@@ -437,7 +448,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         }
     } else if (warp == MMA_WARP) {
         if (lane == 0) {
-            const uint32_t idesc = umma::make_idesc_bf16(TILE_M, N);
+            const uint32_t idesc = umma::make_idesc_bf16(TILE_M, N, MN, MN);
             uint32_t it = 0, j = 0;
             bool ok = true;
             for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++j) {
@@ -454,9 +465,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                     umma::fence_after_sync();
                     const uint32_t sa = umma::smem_u32(smem + s * stage_bytes), sb = sa + a_bytes;
 #pragma unroll
-                    for (int k = 0; k < TILE_K / 16; ++k)
-                        umma::mma_bf16(d, umma::make_desc_sw128(sa + 32u * k), umma::make_desc_sw128(sb + 32u * k),
-                                       idesc, (c > 0 || k > 0) ? 1u : 0u);
+                    for (int k = 0; k < TILE_K / 16; ++k) {
+                        const uint64_t ad = MN ? umma::make_desc_sw128_mn(sa + 2048u * k, 8192u)
+                                               : umma::make_desc_sw128(sa + 32u * k);
+                        const uint64_t bd = MN ? umma::make_desc_sw128_mn(sb + 2048u * k, 8192u)
+                                               : umma::make_desc_sw128(sb + 32u * k);
+                        umma::mma_bf16(d, ad, bd, idesc, (c > 0 || k > 0) ? 1u : 0u);
+                    }
                     umma::commit(&empty[s]);
                 }
                 if (!ok) break;
@@ -535,6 +550,20 @@ bool make_map(CUtensorMap* m, const bf16* base, int64_t rows, int64_t K, int64_t
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// MN-major operand map: a K x MN BF16 matrix stored row by row (row stride ld
+// elements), boxes of 64 MN-elements x 64 K-rows with the 128-byte swizzle.
+bool make_map_mn(CUtensorMap* m, const bf16* base, int64_t k_rows, int64_t mn, int64_t ld)
+{
+    if (!encoder() || ((uintptr_t)base & 15) || (ld * 2) % 16 || mn % 64 || k_rows % TILE_K || ld < mn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)mn, (cuuint64_t)k_rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+    const cuuint32_t box[2] = {64, 64};
+    const cuuint32_t estr[2] = {1, 1};
+    return g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Store map of a rows x cols BF16 matrix with row stride ld (elements): boxes
 // of 32 x 32 with the 64-byte swizzle of the epilogue's staging tiles.
 bool make_store_map(CUtensorMap* m, const bf16* base, int64_t rows, int64_t cols, int64_t ld)
@@ -550,7 +579,8 @@ bool make_store_map(CUtensorMap* m, const bf16* base, int64_t rows, int64_t cols
                     CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// A [M][K] (row stride lda), B [N][K] (row stride ldb).
+// A [M][K] (row stride lda), B [N][K] (row stride ldb); for EPI_WGRAD A [K][M]
+// and B [K][N] (MN-major, N % 64 == 0).
 template <int EPI>
 int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int grid_x,
                 int splits, cudaStream_t st)
@@ -560,7 +590,11 @@ int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, in
         (int64_t)splits * g.k_split < g.K || grid_x < 1)
         return CL_ERR_ARG;
     CUtensorMap ta, tb;
-    if (!make_map(&ta, A, g.M, g.K, lda, TILE_M) || !make_map(&tb, B, g.N, g.K, ldb, g.N)) return CL_ERR_ARG;
+    if (EPI == EPI_WGRAD) {
+        if (g.N % 64 || !make_map_mn(&ta, A, g.K, g.M, lda) || !make_map_mn(&tb, B, g.K, g.N, ldb)) return CL_ERR_ARG;
+    } else if (!make_map(&ta, A, g.M, g.K, lda, TILE_M) || !make_map(&tb, B, g.N, g.K, ldb, g.N)) {
+        return CL_ERR_ARG;
+    }
     // output maps of the staged epilogues (unused ones are copies of ta)
     OutMaps om;
     om.h = om.ht = om.z = ta;
@@ -568,7 +602,6 @@ int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, in
         if (!g.out_h || !make_store_map(&om.h, g.out_h, g.M, g.N, g.ldh)) return CL_ERR_ARG;
         if (g.out_ht && !make_store_map(&om.ht, g.out_ht, g.N, g.M, g.ldht)) return CL_ERR_ARG;
         if (EPI == EPI_BIAS_SILU && g.out_z && !make_store_map(&om.z, g.out_z, g.M, g.N, g.ldh)) return CL_ERR_ARG;
-        if ((EPI == EPI_LOSS || EPI == EPI_DSILU) && !g.out_ht) return CL_ERR_ARG;
     }
     // the shared-memory opt-in is a per-device attribute of the kernel: set it
     // once for every device this process launches on
@@ -730,9 +763,8 @@ struct cl_mlp {
     // activations and gradients (max_batch rows)
     float *xb = nullptr, *o = nullptr;
     int32_t* brow = nullptr;        // training-set row of each minibatch row
-    bf16 *h1 = nullptr, *h1t = nullptr, *h2 = nullptr, *h2t = nullptr, *z2 = nullptr;
-    bf16 *h3 = nullptr, *h3t = nullptr, *z3 = nullptr;
-    bf16 *dO = nullptr, *dOt = nullptr, *dz3 = nullptr, *dz3t = nullptr, *dz2 = nullptr, *dz2t = nullptr;
+    bf16 *h1 = nullptr, *h2 = nullptr, *z2 = nullptr, *h3 = nullptr, *z3 = nullptr;
+    bf16 *dO = nullptr, *dz3 = nullptr, *dz2 = nullptr;
     float* loss = nullptr;          // device accumulator
     unsigned int* derr = nullptr;
     // training set (device pointers owned by the caller)
@@ -786,23 +818,22 @@ GemmArgs gemm_args(cl_mlp* m)
 }
 
 // Forward pass over B rows of m->xb (B % 128 == 0).  Training (with_loss):
-// keeps Z, H^T for the backward pass and ends in the loss epilogue, which
+// keeps H and Z for the backward pass and ends in the loss epilogue, which
 // reads the targets (rows `trow` of `target`, or its first B rows) and writes
-// dO, dO^T, the b4 gradient and the loss.  Inference: O into m->o.
+// dO, the b4 gradient and the loss.  Inference: O into m->o.
 int forward(cl_mlp* m, int B, bool with_loss, const float* target, const int32_t* trow, cudaStream_t st)
 {
     const int grid = grid_for(m, B);
     if (with_loss) cudaMemsetAsync(m->g, 0, N_PARAMS * sizeof(float), st);
-    layer1_fwd<<<(unsigned)(B / L1_ROWS), 256, 0, st>>>(m->xb, m->p + OFF_W1, m->p + OFF_B1, B, m->h1,
-                                                         with_loss ? m->h1t : nullptr);
+    layer1_fwd<<<(unsigned)(B / L1_ROWS), 256, 0, st>>>(m->xb, m->p + OFF_W1, m->p + OFF_B1, B, m->h1, nullptr);
     GemmArgs g = gemm_args(m);
     g.M = B; g.N = D_H; g.K = D_H; g.k_split = D_H;
     g.bias = m->p + OFF_B2; g.out_h = m->h2; g.ldh = D_H;
-    g.out_ht = with_loss ? m->h2t : nullptr; g.ldht = B; g.out_z = with_loss ? m->z2 : nullptr;
+    g.out_z = with_loss ? m->z2 : nullptr;
     int rc = launch_gemm<EPI_BIAS_SILU>(g, m->h1, D_H, m->w2t, D_H, grid, 1, st);
     if (rc) return rc;
     g.bias = m->p + OFF_B3; g.out_h = m->h3;
-    g.out_ht = with_loss ? m->h3t : nullptr; g.out_z = with_loss ? m->z3 : nullptr;
+    g.out_z = with_loss ? m->z3 : nullptr;
     if ((rc = launch_gemm<EPI_BIAS_SILU>(g, m->h2, D_H, m->w3t, D_H, grid, 1, st))) return rc;
     GemmArgs q = gemm_args(m);
     q.M = B; q.N = D_OUT; q.K = D_H; q.k_split = D_H; q.bias = m->p + OFF_B4;
@@ -811,7 +842,7 @@ int forward(cl_mlp* m, int B, bool with_loss, const float* target, const int32_t
         return launch_gemm<EPI_BIAS_F32>(q, m->h3, D_H, m->w4t, D_H, grid, 1, st);
     }
     q.target = target; q.trow = trow; q.scale = 1.0f / ((float)B * (float)D_OUT); q.loss = m->loss;
-    q.out_h = m->dO; q.ldh = D_OUT; q.out_ht = m->dOt; q.ldht = B; q.colsum = m->g + OFF_B4;
+    q.out_h = m->dO; q.ldh = D_OUT; q.colsum = m->g + OFF_B4;
     return launch_gemm<EPI_LOSS>(q, m->h3, D_H, m->w4t, D_H, grid, 1, st);
 }
 
@@ -824,11 +855,11 @@ int backward(cl_mlp* m, int B, cudaStream_t st)
     // backward data: dZ3 = (dO W4) * silu'(Z3), dZ2 = (dZ3 W3) * silu'(Z2), dZ1 = (dZ2 W2) * silu'(Z1)
     GemmArgs g = gemm_args(m);
     g.M = B; g.N = D_H; g.K = D_OUT; g.k_split = D_OUT;
-    g.out_h = m->dz3; g.ldh = D_H; g.out_ht = m->dz3t; g.ldht = B; g.zprev = m->z3; g.colsum = m->g + OFF_B3;
+    g.out_h = m->dz3; g.ldh = D_H; g.zprev = m->z3; g.colsum = m->g + OFF_B3;
     int rc = launch_gemm<EPI_DSILU>(g, m->dO, D_OUT, m->w4, D_OUT, grid, 1, st);
     if (rc) return rc;
     g.K = D_H; g.k_split = D_H;
-    g.out_h = m->dz2; g.out_ht = m->dz2t; g.zprev = m->z2; g.colsum = m->g + OFF_B2;
+    g.out_h = m->dz2; g.zprev = m->z2; g.colsum = m->g + OFF_B2;
     if ((rc = launch_gemm<EPI_DSILU>(g, m->dz3, D_H, m->w3, D_H, grid, 1, st))) return rc;
     GemmArgs l1 = gemm_args(m);
     l1.M = B; l1.N = D_H; l1.K = D_H; l1.k_split = D_H;
@@ -838,13 +869,13 @@ int backward(cl_mlp* m, int B, cudaStream_t st)
     // weight gradients dW = H^T dZ (split-K over the batch), each split added
     // in place into grad W^T (zeroed by the forward pass)
     const int splits = (B + WGRAD_SPLIT_K - 1) / WGRAD_SPLIT_K;
-    struct WG { const bf16* ht; const bf16* dzt; int OUT; int64_t off_w; };
-    const WG wg[3] = {{m->h3t, m->dOt, D_OUT, OFF_W4}, {m->h2t, m->dz3t, D_H, OFF_W3}, {m->h1t, m->dz2t, D_H, OFF_W2}};
+    struct WG { const bf16* h; const bf16* dz; int OUT; int64_t off_w; };
+    const WG wg[3] = {{m->h3, m->dO, D_OUT, OFF_W4}, {m->h2, m->dz3, D_H, OFF_W3}, {m->h1, m->dz2, D_H, OFF_W2}};
     for (int l = 0; l < 3; ++l) {
         GemmArgs w = gemm_args(m);
         w.M = D_H; w.N = wg[l].OUT; w.K = B; w.k_split = WGRAD_SPLIT_K;
         w.out_f = m->g + wg[l].off_w; w.ldf = D_H;
-        if ((rc = launch_gemm<EPI_WGRAD>(w, wg[l].ht, B, wg[l].dzt, B, D_H / TILE_M, splits, st))) return rc;
+        if ((rc = launch_gemm<EPI_WGRAD>(w, wg[l].h, D_H, wg[l].dz, wg[l].OUT, D_H / TILE_M, splits, st))) return rc;
     }
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
 }
@@ -895,12 +926,10 @@ int cl_mlp_create(cl_mlp** out, int device, int max_batch)
               dalloc(m, &m->w3t, (size_t)D_H * D_H) && dalloc(m, &m->w3, (size_t)D_H * D_H) &&
               dalloc(m, &m->w4t, (size_t)D_OUT * D_H) && dalloc(m, &m->w4, (size_t)D_OUT * D_H) &&
               dalloc(m, &m->xb, B * D_IN) && dalloc(m, &m->brow, B) && dalloc(m, &m->o, B * D_OUT) &&
-              dalloc(m, &m->h1, B * D_H) && dalloc(m, &m->h1t, B * D_H) &&
-              dalloc(m, &m->h2, B * D_H) && dalloc(m, &m->h2t, B * D_H) && dalloc(m, &m->z2, B * D_H) &&
-              dalloc(m, &m->h3, B * D_H) && dalloc(m, &m->h3t, B * D_H) && dalloc(m, &m->z3, B * D_H) &&
-              dalloc(m, &m->dO, B * D_OUT) && dalloc(m, &m->dOt, B * D_OUT) &&
-              dalloc(m, &m->dz3, B * D_H) && dalloc(m, &m->dz3t, B * D_H) &&
-              dalloc(m, &m->dz2, B * D_H) && dalloc(m, &m->dz2t, B * D_H) &&
+              dalloc(m, &m->h1, B * D_H) &&
+              dalloc(m, &m->h2, B * D_H) && dalloc(m, &m->z2, B * D_H) &&
+              dalloc(m, &m->h3, B * D_H) && dalloc(m, &m->z3, B * D_H) &&
+              dalloc(m, &m->dO, B * D_OUT) && dalloc(m, &m->dz3, B * D_H) && dalloc(m, &m->dz2, B * D_H) &&
               dalloc(m, &m->loss, 1) &&
               dalloc(m, &m->derr, 1);
     if (!ok) {

@@ -64,12 +64,29 @@ __device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr)
     return d;
 }
 
-// 32-bit instruction descriptor for kind::f16: D = F32 (bits 4-5 = 1),
-// A = B = BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 in bits 17-22,
-// M >> 4 in bits 24-28.
-__host__ __device__ constexpr uint32_t make_idesc_bf16(int M, int N)
+// Descriptor of a 128-byte-swizzled MN-major tile, as TMA writes boxes of
+// 64 MN-elements (128 bytes) x 64 K-rows: swizzle atoms of 64 MN-elements x
+// 8 K-rows (1 KB), consecutive 8-row K groups SBO = 1024 bytes apart,
+// consecutive 64-element MN groups LBO bytes apart (the box size, 8 KB); a K
+// step of 16 advances the start address by two atoms (2 KB).
+__device__ __forceinline__ uint64_t make_desc_sw128_mn(uint32_t saddr, uint32_t lbo_bytes)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// 32-bit instruction descriptor for kind::f16: D = F32 (bits 4-5 = 1),
+// A = B = BF16 (bits 7-9, 10-12 = 1), A and B K-major (0) or MN-major (1) in
+// bits 15 and 16, N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t make_idesc_bf16(int M, int N, bool a_mn = false, bool b_mn = false)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 // D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread.
