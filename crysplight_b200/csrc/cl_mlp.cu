@@ -2,21 +2,23 @@
 // MLP trained and evaluated on sm_100a by hand-written kernels.
 //
 // GEMMs run on the 5th-generation tensor cores: BF16 operands streamed by TMA
-// into a 2- to 4-stage shared-memory ring (128-byte swizzled K-major tiles),
-// one thread issuing tcgen05.mma into a double-buffered FP32 accumulator in
-// tensor memory, and sixteen warps draining it through fused epilogues (bias,
-// SiLU, SiLU', the loss and its gradient, bias-gradient column sums, the
-// layer-1 gradients, BF16 casts, transposed copies, split-K partials).  The
-// 3-wide input layer, the split-K reduction and Adam run on the CUDA cores.
+// into a 3- or 4-stage shared-memory ring (128-byte swizzled tiles, K-major,
+// or MN-major for the weight gradients, which read the activations and
+// gradients as stored), one thread issuing tcgen05.mma into a double-buffered
+// FP32 accumulator in tensor memory, and sixteen warps draining it through
+// fused epilogues (bias, SiLU, SiLU', the loss and its gradient, bias-gradient
+// column sums, the layer-1 gradients, BF16 casts, weight-gradient splits
+// added in place).  The 3-wide input layer and Adam run on the CUDA cores.
 // The epilogues are element-wise work over the 128 x N accumulator of every
 // tile; they are spread over sixteen warps (four per TMEM lane quadrant, each
 // taking every fourth 32-column chunk) so that draining a tile keeps pace
 // with the tensor cores filling the other accumulator.  Their BF16 outputs
-// (row-major and transposed) are staged in shared memory as 32 x 32 tiles and
-// written by TMA stores: stored straight from registers, each 16-byte store
-// of a warp touched 32 rows, and the store queue, not the arithmetic, set the
-// pace.  The per-column constants they read (biases, the layer-1 weights) are
-// staged in shared memory once per CTA.
+// are staged in shared memory as 32 x 32 tiles and written by TMA stores:
+// stored straight from registers, each 16-byte store of a warp touched 32
+// rows, and the store queue, not the arithmetic, set the pace.  Column sums
+// go through a transposed staging tile into per-CTA shared accumulators (one
+// global atomic per column and CTA).  The per-column constants the epilogues
+// read (biases, the layer-1 weights) are staged in shared memory once per CTA.
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -55,11 +57,11 @@ constexpr uint32_t WAIT_BUDGET = 1u << 22;   // polls before a wait gives up
 
 enum Epi : int {
     EPI_F32 = 0,         // out_f[m][n] = acc
-    EPI_BIAS_SILU = 1,   // z = acc + b: out_z = bf16(z), out_h = bf16(silu z), out_ht = transposed
+    EPI_BIAS_SILU = 1,   // z = acc + b: out_z = bf16(z), out_h = bf16(silu z)
     EPI_BIAS_F32 = 2,    // out_f[m][n] = acc + b
-    EPI_DSILU = 3,       // g = bf16(acc * silu'(zprev)): out_h, out_ht, colsum += column sums of g
+    EPI_DSILU = 3,       // g = bf16(acc * silu'(zprev)): out_h, colsum += column sums of g
     EPI_PARTIAL = 4,     // out_f[split][m][n] = acc (split-K partial)
-    EPI_LOSS = 5,        // o = acc + b, d = o - target: loss += scale d^2, g = bf16(2 scale d) -> out_h, out_ht, colsum
+    EPI_LOSS = 5,        // o = acc + b, d = o - target: loss += scale d^2, g = bf16(2 scale d) -> out_h, colsum
     EPI_DSILU_L1 = 6,    // as EPI_DSILU with zprev recomputed from x, W1, b1; colsum and gw1 += g, g x
     EPI_WGRAD = 7,       // out_f[n][m] += acc (a K split of a weight gradient, added in place, transposed);
                          // A [K][M] and B [K][N] MN-major (the activations and gradients as stored)
@@ -72,9 +74,9 @@ enum Epi : int {
 // in shared memory (bias; for EPI_DSILU_L1 also W1 by input component).
 template <int EPI>
 struct EpiCfg {
-    static constexpr int tiles = EPI == EPI_BIAS_SILU ? 3 : (EPI == EPI_LOSS || EPI == EPI_DSILU) ? 2
-                                                          : EPI == EPI_DSILU_L1 ? 1 : 0;
-    static constexpr int stages = EPI == EPI_BIAS_SILU ? 2 : (tiles ? 3 : 4);
+    static constexpr int tiles = (EPI == EPI_BIAS_SILU || EPI == EPI_LOSS || EPI == EPI_DSILU) ? 2
+                                 : EPI == EPI_DSILU_L1 ? 1 : 0;
+    static constexpr int stages = tiles ? 3 : 4;
     static constexpr bool bias = EPI == EPI_BIAS_SILU || EPI == EPI_BIAS_F32 || EPI == EPI_LOSS ||
                                  EPI == EPI_DSILU_L1;
     static constexpr int cst = EPI == EPI_DSILU_L1 ? 4 * 256 : (bias ? 256 : 4);
@@ -98,7 +100,6 @@ struct GemmArgs {
     const float* bias;
     float* out_f; int64_t ldf;
     bf16* out_h; int64_t ldh;       // [M][N]
-    bf16* out_ht; int64_t ldht;     // [N][M]
     bf16* out_z;                    // [M][N], ld = ldh
     const bf16* zprev;              // [M][N], ld = ldh
     const float* target;            // EPI_LOSS: FP32 rows of N targets
@@ -155,8 +156,8 @@ __device__ __forceinline__ void stage_done()
     __syncwarp();
 }
 
-// Eight consecutive per-column constants (or row inputs) from shared memory (all lanes read
-// the same address: a broadcast).
+// Eight consecutive per-column constants (or row inputs) from shared memory
+// (all lanes read the same address: a broadcast).
 __device__ __forceinline__ void cst8(const float* c, float* o)
 {
     const float4 p = reinterpret_cast<const float4*>(c)[0], q = reinterpret_cast<const float4*>(c)[1];
@@ -191,11 +192,11 @@ __device__ __forceinline__ void warp_col_sums(const uint8_t* tt, int lane, float
     }
 }
 
-// TMA output maps of a GEMM: the row-major output (out_h), its transpose
-// (out_ht) and the pre-activations (out_z), boxes of 32 x 32 BF16 with the
-// 64-byte swizzle; maps of absent outputs are unused copies.
+// TMA output maps of a GEMM: the row-major output (out_h) and the
+// pre-activations (out_z), boxes of 32 x 32 BF16 with the 64-byte swizzle;
+// maps of absent outputs are unused copies.
 struct OutMaps {
-    CUtensorMap h, ht, z;
+    CUtensorMap h, z;
 };
 
 // Epilogue of one 128 x N tile: the warp owns rows row0 + lane (row0 = tile
@@ -208,10 +209,15 @@ struct OutMaps {
 template <int EPI>
 __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, uint32_t tbase, int row0,
                                          int lane, int half, const float* cst, uint8_t* stg, bool& pending,
-                                         float* acc)
+                                         float* acc, int next_row0)
 {
     const int N = G.N;
     const int row = row0 + lane;
+    // the rows of this warp's next tile, whose epilogue inputs are brought
+    // into L2 once this tile is done (next_row0 < 0: no next tile)
+    int64_t next_in = -1;
+    if ((EPI == EPI_LOSS || EPI == EPI_DSILU) && next_row0 >= 0)
+        next_in = EPI == EPI_LOSS && G.trow ? (int64_t)G.trow[next_row0 + lane] : (int64_t)(next_row0 + lane);
     float sq = 0.0f;
     float* xs = reinterpret_cast<float*>(stg + EpiCfg<EPI>::tiles * STAGE_TILE_BYTES);
     float x0 = 0.f, x1 = 0.f, x2 = 0.f;
@@ -226,16 +232,10 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
             pending = false;
             __syncwarp();
         }
-        // the chunk's global inputs are requested before the accumulator is
-        // read, so that their latency overlaps the tensor-memory load
-        float4 tg[8];
+        // the chunk's pre-activations are requested before the accumulator is
+        // read, so that their latency overlaps the tensor-memory load (the
+        // loss targets come from L2, prefetched during the previous tile)
         uint4 zp4[4];
-        if (EPI == EPI_LOSS) {
-            const int64_t tr = G.trow ? (int64_t)G.trow[row] : (int64_t)row;
-            const float4* t4 = reinterpret_cast<const float4*>(G.target + tr * N + c0);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) tg[i] = t4[i];
-        }
         if (EPI == EPI_DSILU) {
             const uint4* z4 = reinterpret_cast<const uint4*>(G.zprev + (int64_t)row * G.ldh + c0);
 #pragma unroll
@@ -277,13 +277,11 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
                 }
             }
             stage_row(stg, lane, h);
-            if (G.out_ht) stage_col(stg + STAGE_TILE_BYTES, lane, h);
-            if (G.out_z) stage_row(stg + 2 * STAGE_TILE_BYTES, lane, zz);
+            if (G.out_z) stage_row(stg + STAGE_TILE_BYTES, lane, zz);
             stage_done();
             if (lane == 0) {
                 umma::tma_store_2d(&om.h, c0, row0, stg);
-                if (G.out_ht) umma::tma_store_2d(&om.ht, row0, c0, stg + STAGE_TILE_BYTES);
-                if (G.out_z) umma::tma_store_2d(&om.z, c0, row0, stg + 2 * STAGE_TILE_BYTES);
+                if (G.out_z) umma::tma_store_2d(&om.z, c0, row0, stg + STAGE_TILE_BYTES);
                 umma::bulk_commit();
             }
             pending = true;
@@ -294,7 +292,9 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
                 for (int g = 0; g < 4; ++g) {
                     float b[8];
                     cst8(cst + c0 + 8 * g, b);
-                    const float4 ta = tg[2 * g], tb = tg[2 * g + 1];
+                    const int64_t tr = G.trow ? (int64_t)G.trow[row] : (int64_t)row;
+                    const float4* t4 = reinterpret_cast<const float4*>(G.target + tr * N + c0);
+                    const float4 ta = t4[2 * g], tb = t4[2 * g + 1];
                     const float tt[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
@@ -326,7 +326,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
                     }
                 }
             }
-            // the transposed tile serves the column sums (and out_ht); EPI_DSILU_L1 writes no BF16 output
+            // the transposed tile serves the column sums; EPI_DSILU_L1 writes no BF16 output
             uint8_t* tt = stg + (EPI == EPI_DSILU_L1 ? 0u : STAGE_TILE_BYTES);
             if (EPI != EPI_DSILU_L1) stage_row(stg, lane, h);
             stage_col(tt, lane, h);
@@ -334,7 +334,6 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
             if (EPI != EPI_DSILU_L1) {
                 if (lane == 0) {
                     if (G.out_h) umma::tma_store_2d(&om.h, c0, row0, stg);
-                    if (G.out_ht) umma::tma_store_2d(&om.ht, row0, c0, tt);
                     umma::bulk_commit();
                 }
                 pending = true;
@@ -349,6 +348,13 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
         if (lane == 0) atomicAdd(G.loss, sq * G.scale);
+    }
+    if ((EPI == EPI_LOSS || EPI == EPI_DSILU) && next_in >= 0) {
+        for (int c0 = 32 * half; c0 < N; c0 += 32 * (EPI_WARPS / 4)) {
+            const void* p = EPI == EPI_LOSS ? (const void*)(G.target + next_in * N + c0)
+                                            : (const void*)(G.zprev + next_in * G.ldh + c0);
+            asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
+        }
     }
 }
 
@@ -401,7 +407,6 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         umma::prefetch_tmap(&tmB);
         if (EpiCfg<EPI>::tiles > 0 && EPI != EPI_DSILU_L1) {
             umma::prefetch_tmap(&om.h);
-            umma::prefetch_tmap(&om.ht);
             if (EPI == EPI_BIAS_SILU) umma::prefetch_tmap(&om.z);
         }
     }
@@ -495,8 +500,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             }
             umma::fence_after_sync();
             const int quad = warp & 3;
+            const int next = tile + (int)gridDim.x;
             epilogue<EPI>(G, om, tmem + a * 256u + ((uint32_t)(32 * quad) << 16), tile * TILE_M + 32 * quad,
-                          lane, warp >> 2, s_cst, stg, pending, s_acc);
+                          lane, warp >> 2, s_cst, stg, pending, s_acc,
+                          next < n_tiles ? next * TILE_M + 32 * quad : -1);
             umma::fence_before_sync();
             __syncwarp();
             if (lane == 0) umma::mbar_arrive(&acc_empty[a]);
@@ -597,10 +604,9 @@ int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, in
     }
     // output maps of the staged epilogues (unused ones are copies of ta)
     OutMaps om;
-    om.h = om.ht = om.z = ta;
+    om.h = om.z = ta;
     if (EpiCfg<EPI>::tiles > 0 && EPI != EPI_DSILU_L1) {
         if (!g.out_h || !make_store_map(&om.h, g.out_h, g.M, g.N, g.ldh)) return CL_ERR_ARG;
-        if (g.out_ht && !make_store_map(&om.ht, g.out_ht, g.N, g.M, g.ldht)) return CL_ERR_ARG;
         if (EPI == EPI_BIAS_SILU && g.out_z && !make_store_map(&om.z, g.out_z, g.M, g.N, g.ldh)) return CL_ERR_ARG;
     }
     // the shared-memory opt-in is a per-device attribute of the kernel: set it
@@ -661,32 +667,27 @@ __global__ void __launch_bounds__(256) gather_batch(const float* __restrict__ X,
 }
 
 // Layer 1 (K = 3) on the CUDA cores: h = silu(x W1^T + b1) for 64 rows per
-// block, one thread per feature; H rows and (optionally) H^T rows go out
-// coalesced through a shared tile.
+// block; a thread takes two adjacent features of every other row, so that a
+// warp stores 128 contiguous bytes of a row per instruction.
 constexpr int L1_ROWS = 64;
 __global__ void __launch_bounds__(256) layer1_fwd(const float* __restrict__ X, const float* __restrict__ W1,
-                                                  const float* __restrict__ b1, int B, bf16* H, bf16* Ht)
+                                                  const float* __restrict__ b1, bf16* H)
 {
     __shared__ float xs[L1_ROWS * 3];
-    __shared__ __align__(16) bf16 hs[D_H][L1_ROWS + 8];
     const int b0 = blockIdx.x * L1_ROWS;
     for (int i = threadIdx.x; i < L1_ROWS * 3; i += blockDim.x) xs[i] = X[(int64_t)b0 * 3 + i];
     __syncthreads();
-    const int j = threadIdx.x;
-    const float w0 = W1[j * 3], w1 = W1[j * 3 + 1], w2 = W1[j * 3 + 2], bj = b1[j];
-    for (int r = 0; r < L1_ROWS; ++r) {
+    const int j = 2 * (threadIdx.x % (D_H / 2)), r0 = threadIdx.x / (D_H / 2);
+    const float wa0 = W1[j * 3], wa1 = W1[j * 3 + 1], wa2 = W1[j * 3 + 2], ba = b1[j];
+    const float wb0 = W1[j * 3 + 3], wb1 = W1[j * 3 + 4], wb2 = W1[j * 3 + 5], bb = b1[j + 1];
+    __nv_bfloat162* out = reinterpret_cast<__nv_bfloat162*>(H + (int64_t)b0 * D_H + j);
+#pragma unroll 4
+    for (int r = r0; r < L1_ROWS; r += 2) {
         // same operations, same order as the layer-1 recompute in the backward epilogue
-        const float z = bj + xs[r * 3] * w0 + xs[r * 3 + 1] * w1 + xs[r * 3 + 2] * w2;
-        const bf16 h = __float2bfloat16_rn(silu(z));
-        H[(int64_t)(b0 + r) * D_H + j] = h;
-        hs[j][r] = h;
-    }
-    if (!Ht) return;
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < D_H * (L1_ROWS / 2); idx += blockDim.x) {
-        const int jj = idx / (L1_ROWS / 2), q = idx % (L1_ROWS / 2);
-        *reinterpret_cast<__nv_bfloat162*>(Ht + (int64_t)jj * B + b0 + 2 * q) =
-            *reinterpret_cast<const __nv_bfloat162*>(&hs[jj][2 * q]);
+        const float x0 = xs[r * 3], x1 = xs[r * 3 + 1], x2 = xs[r * 3 + 2];
+        const float za = ba + x0 * wa0 + x1 * wa1 + x2 * wa2;
+        const float zb = bb + x0 * wb0 + x1 * wb1 + x2 * wb2;
+        out[(int64_t)r * (D_H / 2)] = __floats2bfloat162_rn(silu(za), silu(zb));
     }
 }
 
@@ -825,7 +826,7 @@ int forward(cl_mlp* m, int B, bool with_loss, const float* target, const int32_t
 {
     const int grid = grid_for(m, B);
     if (with_loss) cudaMemsetAsync(m->g, 0, N_PARAMS * sizeof(float), st);
-    layer1_fwd<<<(unsigned)(B / L1_ROWS), 256, 0, st>>>(m->xb, m->p + OFF_W1, m->p + OFF_B1, B, m->h1, nullptr);
+    layer1_fwd<<<(unsigned)(B / L1_ROWS), 256, 0, st>>>(m->xb, m->p + OFF_W1, m->p + OFF_B1, m->h1);
     GemmArgs g = gemm_args(m);
     g.M = B; g.N = D_H; g.K = D_H; g.k_split = D_H;
     g.bias = m->p + OFF_B2; g.out_h = m->h2; g.ldh = D_H;
