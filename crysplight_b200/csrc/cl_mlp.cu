@@ -97,6 +97,7 @@ __host__ __device__ constexpr size_t gemm_smem_bytes(int N)
 struct GemmArgs {
     int M, N, K;                    // M % 128 == 0, N % 32 == 0 && 32 <= N <= 256, K % 64 == 0
     int k_split;                    // K elements per split (gridDim.y splits)
+    int n_full;                     // row tiles taken whole; the rest go as two N halves each
     const float* bias;
     float* out_f; int64_t ldf;
     bf16* out_h; int64_t ldh;       // [M][N]
@@ -199,6 +200,20 @@ struct OutMaps {
     CUtensorMap h, z;
 };
 
+// A unit of work: row tile `tile`, accumulator columns [n0, n0 + nw).  The
+// first n_full units are whole tiles; the remaining tiles are split into two
+// units of N/2 columns each, so that the last round over the CTAs is half as
+// long (512 tiles on 148 SMs: 3.5 tiles' time instead of 4).
+struct Unit {
+    int tile, n0, nw;
+};
+__device__ __forceinline__ Unit unit_of(int u, int n_full, int N)
+{
+    if (u < n_full) return Unit{u, 0, N};
+    const int v = u - n_full;
+    return Unit{n_full + (v >> 1), (v & 1) * (N >> 1), N >> 1};
+}
+
 // Epilogue of one 128 x N tile: the warp owns rows row0 + lane (row0 = tile
 // row + 32 (w % 4)) and the 32-column chunks c0 = 32 (half + 4 k).  cst holds
 // the bias (and for EPI_DSILU_L1 the columns of W1 at cst + 256 (1 + k)) in
@@ -209,7 +224,7 @@ struct OutMaps {
 template <int EPI>
 __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, uint32_t tbase, int row0,
                                          int lane, int half, const float* cst, uint8_t* stg, bool& pending,
-                                         float* acc, int next_row0)
+                                         float* acc, Unit un, int next_row0, Unit next)
 {
     const int N = G.N;
     const int row = row0 + lane;
@@ -225,7 +240,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
         x0 = G.x[(int64_t)row * 3]; x1 = G.x[(int64_t)row * 3 + 1]; x2 = G.x[(int64_t)row * 3 + 2];
         xs[lane] = x0; xs[32 + lane] = x1; xs[64 + lane] = x2;
     }
-    for (int c0 = 32 * half; c0 < N; c0 += 32 * (EPI_WARPS / 4)) {
+    for (int c0 = un.n0 + 32 * half; c0 < un.n0 + un.nw; c0 += 32 * (EPI_WARPS / 4)) {
         if (EpiCfg<EPI>::tiles) {
             // the previous chunk's TMA stores have read the staging tiles
             if (pending && lane == 0) umma::bulk_wait_read0();
@@ -242,7 +257,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
             for (int i = 0; i < 4; ++i) zp4[i] = z4[i];
         }
         float v[32];
-        umma::tmem_ld32(tbase + (uint32_t)c0, v);
+        umma::tmem_ld32(tbase + (uint32_t)(c0 - un.n0), v);
         if (EPI == EPI_WGRAD) {
             // column n of the tile is row n of the transposed output: the warp's
             // 32 rows are 32 consecutive floats there (one coalesced reduction)
@@ -350,7 +365,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
         if (lane == 0) atomicAdd(G.loss, sq * G.scale);
     }
     if ((EPI == EPI_LOSS || EPI == EPI_DSILU) && next_in >= 0) {
-        for (int c0 = 32 * half; c0 < N; c0 += 32 * (EPI_WARPS / 4)) {
+        for (int c0 = next.n0 + 32 * half; c0 < next.n0 + next.nw; c0 += 32 * (EPI_WARPS / 4)) {
             const void* p = EPI == EPI_LOSS ? (const void*)(G.target + next_in * N + c0)
                                             : (const void*)(G.zprev + next_in * G.ldh + c0);
             asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
@@ -370,7 +385,8 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
 template <int EPI>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                const __grid_constant__ OutMaps om, const __grid_constant__ GemmArgs G)
+                const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ OutMaps om,
+                const __grid_constant__ GemmArgs G)
 {
     constexpr int STAGES = EpiCfg<EPI>::stages;
     constexpr bool MN = EPI == EPI_WGRAD;   // MN-major operands
@@ -392,7 +408,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     const int k_end = min(G.K, k_begin + G.k_split);
     const int n_chunks = (k_end - k_begin) / TILE_K;
     const int n_tiles = G.M / TILE_M;
-    if (n_chunks <= 0 || (int)blockIdx.x >= n_tiles) return;   // uniform over the CTA
+    const int n_units = G.n_full + 2 * (n_tiles - G.n_full);
+    if (n_chunks <= 0 || (int)blockIdx.x >= n_units) return;   // uniform over the CTA
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     volatile int* abort_v = &abort_flag;
@@ -405,6 +422,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     if (warp == PRODUCER_WARP && lane == 0) {
         umma::prefetch_tmap(&tmA);
         umma::prefetch_tmap(&tmB);
+        if (G.n_full < n_tiles) umma::prefetch_tmap(&tmBh);
         if (EpiCfg<EPI>::tiles > 0 && EPI != EPI_DSILU_L1) {
             umma::prefetch_tmap(&om.h);
             if (EPI == EPI_BIAS_SILU) umma::prefetch_tmap(&om.z);
@@ -424,7 +442,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         if (lane == 0) {
             uint32_t it = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+            for (int ui = blockIdx.x; ui < n_units && ok; ui += gridDim.x) {
+                const Unit un = unit_of(ui, G.n_full, N);
+                const int tile = un.tile;
                 for (int c = 0; c < n_chunks; ++c, ++it) {
                     const uint32_t s = it % STAGES, r = it / STAGES;
                     if (r > 0 && !umma::mbar_wait_or_abort(&empty[s], (r - 1) & 1u, WAIT_BUDGET, abort_v)) {
@@ -432,7 +452,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                         break;
                     }
                     uint8_t* st = smem + s * stage_bytes;
-                    umma::mbar_arrive_expect_tx(&full[s], stage_bytes);
+                    umma::mbar_arrive_expect_tx(&full[s], a_bytes + (uint32_t)un.nw * 128u);
                     const int k0 = k_begin + c * TILE_K;
                     if (MN) {
                         // boxes of 64 MN-elements x 64 K-rows, 8 KB apart
@@ -442,7 +462,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                             umma::tma_load_2d(st + a_bytes + 8192 * q, &tmB, 64 * q, k0, &full[s]);
                     } else {
                         umma::tma_load_2d(st, &tmA, k0, tile * TILE_M, &full[s]);
-                        umma::tma_load_2d(st + a_bytes, &tmB, k0, 0, &full[s]);
+                        if (un.nw == N) umma::tma_load_2d(st + a_bytes, &tmB, k0, 0, &full[s]);
+                        else umma::tma_load_2d(st + a_bytes, &tmBh, k0, un.n0, &full[s]);
                     }
                 }
             }
@@ -453,10 +474,12 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         }
     } else if (warp == MMA_WARP) {
         if (lane == 0) {
-            const uint32_t idesc = umma::make_idesc_bf16(TILE_M, N, MN, MN);
+            const uint32_t idesc_full = umma::make_idesc_bf16(TILE_M, N, MN, MN);
+            const uint32_t idesc_half = umma::make_idesc_bf16(TILE_M, N / 2, MN, MN);
             uint32_t it = 0, j = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x, ++j) {
+            for (int ui = blockIdx.x; ui < n_units && ok; ui += gridDim.x, ++j) {
+                const uint32_t idesc = ui < G.n_full ? idesc_full : idesc_half;
                 const uint32_t a = j & 1u, u = j >> 1;
                 if (u > 0 && !umma::mbar_wait_or_abort(&acc_empty[a], (u - 1) & 1u, WAIT_BUDGET, abort_v)) {
                     ok = false;
@@ -491,8 +514,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                                                 (EPI == EPI_DSILU_L1 ? XS_BYTES : 0u));
         bool pending = false;   // TMA stores of this warp not yet known to have read its tiles
         uint32_t j = 0;
-        for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++j) {
+        for (int ui = blockIdx.x; ui < n_units; ui += gridDim.x, ++j) {
             const uint32_t a = j & 1u, u = j >> 1;
+            const Unit un = unit_of(ui, G.n_full, N);
             if (!umma::mbar_wait_or_abort(&acc_full[a], u & 1u, WAIT_BUDGET, abort_v)) {
                 if (lane == 0) atomicOr(G.err, 1u);
                 *abort_v = 1;
@@ -500,10 +524,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             }
             umma::fence_after_sync();
             const int quad = warp & 3;
-            const int next = tile + (int)gridDim.x;
-            epilogue<EPI>(G, om, tmem + a * 256u + ((uint32_t)(32 * quad) << 16), tile * TILE_M + 32 * quad,
-                          lane, warp >> 2, s_cst, stg, pending, s_acc,
-                          next < n_tiles ? next * TILE_M + 32 * quad : -1);
+            const int nu = ui + (int)gridDim.x;
+            const Unit next = unit_of(nu < n_units ? nu : ui, G.n_full, N);
+            epilogue<EPI>(G, om, tmem + a * 256u + ((uint32_t)(32 * quad) << 16), un.tile * TILE_M + 32 * quad,
+                          lane, warp >> 2, s_cst, stg, pending, s_acc, un,
+                          nu < n_units ? next.tile * TILE_M + 32 * quad : -1, next);
             umma::fence_before_sync();
             __syncwarp();
             if (lane == 0) umma::mbar_arrive(&acc_empty[a]);
@@ -623,9 +648,19 @@ int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, in
     }
     const int tiles = g.M / TILE_M;
     dim3 grid((unsigned)(grid_x < tiles ? grid_x : tiles), (unsigned)splits);
+    // a last round that would occupy at most half of the CTAs runs as N halves
+    // (two units per tile) on all of them
+    GemmArgs ga = g;
+    ga.n_full = tiles;
+    CUtensorMap tbh = tb;
+    const int r = tiles % (int)grid.x;
+    if (EPI != EPI_WGRAD && EPI != EPI_PARTIAL && splits == 1 && g.N % 64 == 0 && r > 0 && 2 * r <= (int)grid.x) {
+        if (!make_map(&tbh, B, g.N, g.K, ldb, g.N / 2)) return CL_ERR_ARG;
+        ga.n_full = tiles - r;
+    }
     // at least 116 KB so that one CTA holds an SM: each allocates all 512 TMEM columns
     const size_t smem = gemm_smem_bytes<EPI>(g.N) > 116 * 1024 ? gemm_smem_bytes<EPI>(g.N) : 116 * 1024;
-    gemm_kernel<EPI><<<grid, GEMM_THREADS, smem, st>>>(ta, tb, om, g);
+    gemm_kernel<EPI><<<grid, GEMM_THREADS, smem, st>>>(ta, tb, tbh, om, ga);
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
 }
 
@@ -635,7 +670,7 @@ int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, in
 // FP32 accumulation and FP32 master weights with Adam.
 // ===========================================================================
 constexpr int D_IN = 3, D_H = 256, D_OUT = 192;
-constexpr int WGRAD_SPLIT_K = 1024;      // batch rows per weight-gradient split
+constexpr int WGRAD_MIN_SPLIT_K = 512;   // fewest batch rows per weight-gradient split
 
 __device__ __forceinline__ uint32_t hash32(uint32_t a, uint32_t b, uint32_t c)
 {
@@ -869,12 +904,16 @@ int backward(cl_mlp* m, int B, cudaStream_t st)
     if ((rc = launch_gemm<EPI_DSILU_L1>(l1, m->dz2, D_H, m->w2, D_H, grid, 1, st))) return rc;
     // weight gradients dW = H^T dZ (split-K over the batch), each split added
     // in place into grad W^T (zeroed by the forward pass)
-    const int splits = (B + WGRAD_SPLIT_K - 1) / WGRAD_SPLIT_K;
+    // K splits sized so that the two 128-row tiles of the 256 inputs fill every SM once
+    const int per_tile_ctas = m->num_sms / (D_H / TILE_M) > 0 ? m->num_sms / (D_H / TILE_M) : 1;
+    int k_split = ((B + per_tile_ctas - 1) / per_tile_ctas + TILE_K - 1) / TILE_K * TILE_K;
+    if (k_split < WGRAD_MIN_SPLIT_K) k_split = WGRAD_MIN_SPLIT_K;
+    const int splits = (B + k_split - 1) / k_split;
     struct WG { const bf16* h; const bf16* dz; int OUT; int64_t off_w; };
     const WG wg[3] = {{m->h3, m->dO, D_OUT, OFF_W4}, {m->h2, m->dz3, D_H, OFF_W3}, {m->h1, m->dz2, D_H, OFF_W2}};
     for (int l = 0; l < 3; ++l) {
         GemmArgs w = gemm_args(m);
-        w.M = D_H; w.N = wg[l].OUT; w.K = B; w.k_split = WGRAD_SPLIT_K;
+        w.M = D_H; w.N = wg[l].OUT; w.K = B; w.k_split = k_split;
         w.out_f = m->g + wg[l].off_w; w.ldf = D_H;
         if ((rc = launch_gemm<EPI_WGRAD>(w, wg[l].h, D_H, wg[l].dz, wg[l].OUT, D_H / TILE_M, splits, st))) return rc;
     }
