@@ -937,7 +937,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
     ap.add_argument("--workload", choices=("scan256", "point1m", "events_csitl",
-                                           "events_bgo_surrogate"),
+                                           "events_bgo_surrogate", "surrogate_training"),
                     default="scan256")
     ap.add_argument("--events", type=int, default=50_000,
                     help="events in the secondary events/s measurement of the default run "
@@ -980,6 +980,19 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "events_bgo_surrogate":
         run_surrogate_events_arm(args, rank, world, local_rank)
+        return
+    if args.workload == "surrogate_training":
+        # the training leg alone (its line is also part of the default run)
+        if rank != 0:
+            return
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the surrogate has no counterpart "
+                              "in the reference"}))
+            return
+        import torch
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        print(json.dumps(surrogate_training_bench(dev, steps=args.steps, warmup=args.warmup)))
         return
     if args.workload == "events_csitl":
         if world > 1 and args.impl == "cuda":

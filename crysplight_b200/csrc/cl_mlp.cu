@@ -42,6 +42,31 @@ namespace mlp {
 
 using bf16 = __nv_bfloat16;
 
+// Programmatic dependent launch: the kernels of a training step are launched
+// so that the next one may be scheduled while the previous one drains; each
+// kernel allows that at its start (pdl_trigger) and waits for the previous
+// kernel's completion and memory (pdl_wait) before its first global access.
+// Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Launches kernel k with the programmatic-serialization attribute on stream st.
+template <typename... P, typename... A>
+cudaError_t launch_pdl(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, static_cast<P>(args)...);
+}
+
 constexpr int TILE_M = 128;     // rows per CTA tile (TMEM lanes)
 constexpr int TILE_K = 64;      // K elements per pipeline stage (one 128-byte swizzle row)
 #ifndef CL_MLP_EPI_WARPS
@@ -409,6 +434,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     const int n_chunks = (k_end - k_begin) / TILE_K;
     const int n_tiles = G.M / TILE_M;
     const int n_units = G.n_full + 2 * (n_tiles - G.n_full);
+    pdl_trigger();
     if (n_chunks <= 0 || (int)blockIdx.x >= n_units) return;   // uniform over the CTA
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -428,6 +454,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             if (EPI == EPI_BIAS_SILU) umma::prefetch_tmap(&om.z);
         }
     }
+    // barriers, TMEM and tensor-map prefetches above overlap the previous kernel's tail
+    pdl_wait();
     if (EpiCfg<EPI>::bias)
         for (int i = threadIdx.x; i < N; i += blockDim.x) s_cst[i] = G.bias[i];
     if (EPI == EPI_DSILU_L1)
@@ -660,7 +688,8 @@ int launch_gemm(const GemmArgs& g, const bf16* A, int64_t lda, const bf16* B, in
     }
     // at least 116 KB so that one CTA holds an SM: each allocates all 512 TMEM columns
     const size_t smem = gemm_smem_bytes<EPI>(g.N) > 116 * 1024 ? gemm_smem_bytes<EPI>(g.N) : 116 * 1024;
-    gemm_kernel<EPI><<<grid, GEMM_THREADS, smem, st>>>(ta, tb, tbh, om, ga);
+    if (launch_pdl(gemm_kernel<EPI>, grid, dim3(GEMM_THREADS), smem, st, ta, tb, tbh, om, ga) != cudaSuccess)
+        return CL_ERR_CUDA;
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
 }
 
@@ -692,6 +721,8 @@ __device__ __forceinline__ uint32_t hash32(uint32_t a, uint32_t b, uint32_t c)
 __global__ void __launch_bounds__(256) gather_batch(const float* __restrict__ X, int64_t n_all, int B,
                                                     uint32_t seed, uint32_t step, float* Xb, int32_t* rows)
 {
+    pdl_trigger();
+    pdl_wait();
     const int b = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     if (b >= B) return;
     const int64_t i = (int64_t)(hash32((uint32_t)b, step, seed) % (uint32_t)n_all);
@@ -708,6 +739,8 @@ constexpr int L1_ROWS = 64;
 __global__ void __launch_bounds__(256) layer1_fwd(const float* __restrict__ X, const float* __restrict__ W1,
                                                   const float* __restrict__ b1, bf16* H)
 {
+    pdl_trigger();
+    pdl_wait();
     __shared__ float xs[L1_ROWS * 3];
     const int b0 = blockIdx.x * L1_ROWS;
     for (int i = threadIdx.x; i < L1_ROWS * 3; i += blockDim.x) xs[i] = X[(int64_t)b0 * 3 + i];
@@ -726,22 +759,24 @@ __global__ void __launch_bounds__(256) layer1_fwd(const float* __restrict__ X, c
     }
 }
 
-// Adam on an FP32 master tensor; optional BF16 copies of a [OUT][IN] matrix
-// in both layouts ([OUT][IN] for the forward B operand, [IN][OUT] for the
-// backward-data B operand).
-// Adam over the whole parameter block in one launch; the three weight
-// matrices of the tensor-core layers also get their BF16 copies (W^T as
-// stored and W), described by AdamCopies.
+// Adam over the whole parameter block in one launch (FP32 master weights;
+// the gradient is zeroed as it is read); the three weight matrices of the
+// tensor-core layers also get their BF16 copies (W^T as stored for the
+// forward B operand, W for the backward-data B operand), described by
+// AdamCopies.
 struct AdamCopies {
     int64_t off[3]; int n[3]; int OUT[3]; int IN[3];
     bf16* wt[3]; bf16* w[3];
 };
-__global__ void adam_all(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+__global__ void adam_all(float* __restrict__ w, float* __restrict__ g, float* __restrict__ m,
                          float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps, float bc1,
                          float bc2, const AdamCopies C)
 {
+    pdl_trigger();
+    pdl_wait();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float gi = g[i];
+        g[i] = 0.0f;   // zeroed for the next step's accumulation
         const float mi = b1 * m[i] + (1.0f - b1) * gi;
         const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
         m[i] = mi; v[i] = vi;
@@ -857,11 +892,13 @@ GemmArgs gemm_args(cl_mlp* m)
 // keeps H and Z for the backward pass and ends in the loss epilogue, which
 // reads the targets (rows `trow` of `target`, or its first B rows) and writes
 // dO, the b4 gradient and the loss.  Inference: O into m->o.
-int forward(cl_mlp* m, int B, bool with_loss, const float* target, const int32_t* trow, cudaStream_t st)
+int forward(cl_mlp* m, int B, bool with_loss, const float* target, const int32_t* trow, cudaStream_t st,
+            bool zero_grad = true)
 {
     const int grid = grid_for(m, B);
-    if (with_loss) cudaMemsetAsync(m->g, 0, N_PARAMS * sizeof(float), st);
-    layer1_fwd<<<(unsigned)(B / L1_ROWS), 256, 0, st>>>(m->xb, m->p + OFF_W1, m->p + OFF_B1, m->h1);
+    if (with_loss && zero_grad) cudaMemsetAsync(m->g, 0, N_PARAMS * sizeof(float), st);
+    launch_pdl(layer1_fwd, dim3((unsigned)(B / L1_ROWS)), dim3(256), 0, st, (const float*)m->xb,
+               (const float*)(m->p + OFF_W1), (const float*)(m->p + OFF_B1), m->h1);
     GemmArgs g = gemm_args(m);
     g.M = B; g.N = D_H; g.K = D_H; g.k_split = D_H;
     g.bias = m->p + OFF_B2; g.out_h = m->h2; g.ldh = D_H;
@@ -935,7 +972,8 @@ void adam(cl_mlp* m, float lr, cudaStream_t st)
         c.wt[t] = wts[t]; c.w[t] = ws[t];
     }
     const unsigned grid = (unsigned)((N_PARAMS + 255) / 256);
-    adam_all<<<grid, 256, 0, st>>>(m->p, m->g, m->m, m->v, N_PARAMS, lr, b1, b2, eps, bc1, bc2, c);
+    launch_pdl(adam_all, dim3(grid), dim3(256), 0, st, m->p, m->g, m->m, m->v, (int64_t)N_PARAMS,
+               lr, b1, b2, eps, bc1, bc2, c);
 }
 
 }  // namespace
@@ -1049,10 +1087,13 @@ int cl_mlp_train(cl_mlp* m, int steps, int batch, float lr, uint32_t seed, uint3
     cudaSetDevice(m->device);
     cudaStream_t st = m->stream;
     cudaMemsetAsync(m->loss, 0, sizeof(float), st);
+    // the gradient is zeroed once here and then by each Adam step, so that a
+    // step is an unbroken chain of kernels
+    cudaMemsetAsync(m->g, 0, N_PARAMS * sizeof(float), st);
     for (int s = 0; s < steps; ++s) {
-        gather_batch<<<(batch + 255) / 256, 256, 0, st>>>(m->data_x, m->n_data, batch, seed, step0 + (uint32_t)s,
-                                                          m->xb, m->brow);
-        int rc = forward(m, batch, true, m->data_t, m->brow, st);
+        launch_pdl(gather_batch, dim3((batch + 255) / 256), dim3(256), 0, st, (const float*)m->data_x,
+                   (int64_t)m->n_data, batch, seed, step0 + (uint32_t)s, m->xb, m->brow);
+        int rc = forward(m, batch, true, m->data_t, m->brow, st, false);
         if (!rc) rc = backward(m, batch, st);
         if (rc) return mlp_fail(m, rc, "kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
         adam(m, lr, st);
