@@ -22,7 +22,7 @@ EXPORTS = (
     "cl_run_segments_device", "cl_sync", "cl_last_steps", "cl_set_launch",
     "cl_debug_eval", "cl_run_photons_noalloc", "cl_run_segments_moments_device",
     "cl_run_events_surrogate_device", "cl_surrogate_combine", "cl_debug_sampler",
-    "cl_surrogate_inputs", "cl_set_time_budget",
+    "cl_surrogate_inputs", "cl_set_time_budget", "cl_surrogate_combine_direct", "cl_surrogate_direct",
 )
 
 # Fixed-point scales of cl_run_segments_moments_device (crysplight_cuda.h)
@@ -112,6 +112,13 @@ def _declare(lib: C.CDLL) -> None:
                                          C.POINTER(Readout), C.c_float, C.c_float, C.c_float,
                                          _P, _P, _P, _P, _P, _P]
     lib.cl_surrogate_combine.restype = C.c_int
+    lib.cl_surrogate_combine_direct.argtypes = [_P, C.c_int32, C.c_int64, _P, _P, _P, _P, C.POINTER(Box),
+                                                C.POINTER(Readout), C.c_float, C.c_float, C.c_float,
+                                                _P, _P, _P, _P, _P, _P]
+    lib.cl_surrogate_combine_direct.restype = C.c_int
+    lib.cl_surrogate_direct.argtypes = [_P, C.c_int64, C.POINTER(Box), C.POINTER(OpticalParams),
+                                        C.POINTER(Readout), _P, _P]
+    lib.cl_surrogate_direct.restype = C.c_int
     lib.cl_surrogate_inputs.argtypes = [_P, C.c_int64, C.POINTER(Box), C.c_float, _P, _P]
     lib.cl_surrogate_inputs.restype = C.c_int
     lib.cl_debug_sampler.argtypes = [C.c_int, _P, C.c_int64, C.c_uint64, _P, _P, _P]

@@ -271,6 +271,7 @@ struct CombineArgs {
     const float* y_mean;     // [3 * cells]
     const float* y_std;      // [3 * cells]
     const float* xyz;        // [n][3] mm
+    const float* direct;     // [n][CELLS] first-pass probabilities added to the members' (may be null)
     float L0, L1, L2;
     int32_t front_wrapped;
     float pde, spread_max, wall_min_mm;
@@ -307,8 +308,11 @@ __global__ void __launch_bounds__(CELLS * SITES_PER_CTA) surrogate_combine(const
             }
         }
         const double invK = 1.0 / (double)A.K;
-        const double pm = sum_p * invK;
-        const double var = fmax(sum_p2 * invK - pm * pm, 0.0);
+        const double pr = sum_p * invK;
+        const double var = fmax(sum_p2 * invK - pr * pr, 0.0);
+        // the first-pass term is the same for every member: it adds to the
+        // mean and to the total the spread is relative to, not to the spread
+        const double pm = pr + (A.direct && i < A.n ? (double)A.direct[i * CELLS + c] : 0.0);
         double a = sqrt(var), b = pm;
         for (int o = 16; o > 0; o >>= 1) {
             a += __shfl_down_sync(0xffffffffu, a, o);
@@ -334,6 +338,138 @@ __global__ void __launch_bounds__(CELLS * SITES_PER_CTA) surrogate_combine(const
                 A.spread[i] = spr;
                 A.flag[i] = f;
             }
+        }
+        __syncthreads();
+    }
+}
+
+// First-pass light (the analytic part of the light response): the
+// probability that a photon emitted isotropically at a site reaches the
+// readout face z = Lz without a bulk interaction and crosses into SiPM c
+// there, at PDE 1.  A photon leaving at polar angle theta from the face normal
+// travels h / cos(theta) (h = Lz - z) and survives absorption and Rayleigh
+// scattering with probability exp(-mu h / cos theta), mu = 1/abs_len +
+// 1/rayleigh (the competition of the two exponential path lengths against
+// the face distance); the face transmits it with probability 1 - R(cos
+// theta) (the same Fresnel coefficients, total internal reflection beyond
+// the critical angle); it lands on the circle of radius rho = h tan(theta)
+// about the site's projection, uniformly in azimuth, and is detected by the
+// SiPM whose pixel contains the landing point (pixel c = j nx + i for
+// floor(x / pitch) = i, the last column and row reaching the face edge;
+// landing points off the face belong to a side wall first and are not
+// first-pass light).  So
+//     D_c = 1/(4 pi) int_0^theta_max (1 - R) exp(-mu h / cos theta) sin theta
+//           * (arc of the circle inside pixel c) d theta,
+// with the arcs exact (intersections of the circle with the pixel's column
+// and row strips) and theta by composite Gauss-Legendre quadrature (8 panels
+// of 8 nodes up to the critical angle; 64 threads per site, one per node).
+// The rest of the light response (reflections, scattering) varies slowly
+// over the SiPM plane; a surrogate trained on it learns what the first-pass
+// term's sharp pixel edges would otherwise ask of it.
+namespace {
+// 8-point Gauss-Legendre nodes and weights on [-1, 1] (positive half)
+__constant__ double c_gl_x[4] = {0.1834346424956498, 0.5255324099163290, 0.7966664774136267, 0.9602898564975363};
+__constant__ double c_gl_w[4] = {0.3626837833783620, 0.3137066458778873, 0.2223810344533745, 0.1012285362903763};
+}
+
+struct DirectArgs {
+    const float* xyz;        // [n][3] mm
+    int64_t n;
+    float L0, L1, L2;
+    float n1, n2, mu;        // crystal and coupling indices, attenuation 1/mm
+    float pitch;
+    int32_t nx, ny;
+    float* out;              // [n][CELLS]
+};
+
+constexpr int DIRECT_NODES = 64;
+constexpr int DIRECT_SITES_PER_CTA = 4;
+constexpr float TWO_PI_ARC = 6.283185307179586f;
+
+// Length in [0, 2pi) of the circle's azimuths phi with cos(phi) in [ca, cb]
+// and sin(phi) in [sa, sb] (bounds clamped to [-1, 1]).
+__device__ __forceinline__ float arc_in_box(float ca, float cb, float sa, float sb)
+{
+    ca = fminf(fmaxf(ca, -1.0f), 1.0f); cb = fminf(fmaxf(cb, -1.0f), 1.0f);
+    sa = fminf(fmaxf(sa, -1.0f), 1.0f); sb = fminf(fmaxf(sb, -1.0f), 1.0f);
+    const float aa = acosf(ca), ab = acosf(cb);          // ab <= aa
+    const float x1l = ab, x1h = aa, x2l = TWO_PI_ARC - aa, x2h = TWO_PI_ARC - ab;
+    const float ba = asinf(sa), bb = asinf(sb);          // in [-pi/2, pi/2]
+    float y1l, y1h, y2l = 0.0f, y2h = 0.0f;
+    if (ba >= 0.0f) { y1l = ba; y1h = bb; }
+    else if (bb < 0.0f) { y1l = ba + TWO_PI_ARC; y1h = bb + TWO_PI_ARC; }
+    else { y1l = ba + TWO_PI_ARC; y1h = TWO_PI_ARC; y2h = bb; }
+    const float pi = 0.5f * TWO_PI_ARC;
+    const float y3l = pi - bb, y3h = pi - ba;
+    float arc = 0.0f;
+    arc += fmaxf(0.0f, fminf(x1h, y1h) - fmaxf(x1l, y1l));
+    arc += fmaxf(0.0f, fminf(x1h, y2h) - fmaxf(x1l, y2l));
+    arc += fmaxf(0.0f, fminf(x1h, y3h) - fmaxf(x1l, y3l));
+    arc += fmaxf(0.0f, fminf(x2h, y1h) - fmaxf(x2l, y1l));
+    arc += fmaxf(0.0f, fminf(x2h, y2h) - fmaxf(x2l, y2l));
+    arc += fmaxf(0.0f, fminf(x2h, y3h) - fmaxf(x2l, y3l));
+    return arc;
+}
+
+__global__ void __launch_bounds__(DIRECT_NODES * DIRECT_SITES_PER_CTA) surrogate_direct(const DirectArgs A)
+{
+    __shared__ float acc[DIRECT_SITES_PER_CTA][CELLS];
+    const int q = threadIdx.x % DIRECT_NODES;
+    const int s_loc = threadIdx.x / DIRECT_NODES;
+    // this thread's quadrature node: panel q / 8, node q % 8 (mirror pairs)
+    const int panel = q / 8, k = q % 8;
+    const double gx = k < 4 ? -c_gl_x[3 - k] : c_gl_x[k - 4];
+    const double gw = k < 4 ? c_gl_w[3 - k] : c_gl_w[k - 4];
+    const double n1 = A.n1, n2 = A.n2;
+    const double th_max = n2 < n1 ? asin(n2 / n1) : 0.5 * 3.141592653589793;
+    const double t0 = th_max * panel / 8.0, t1 = th_max * (panel + 1) / 8.0;
+    const double th = t0 + 0.5 * (t1 - t0) * (gx + 1.0);
+    const double c = cos(th), sn = sin(th);
+    // Fresnel transmission at the readout face (as fresnel_q2, in Float64)
+    double T = 0.0;
+    {
+        const double q2 = (n1 / n2) * (n1 / n2);
+        const double sin2t = q2 * (1.0 - c * c);
+        if (sin2t < 1.0) {
+            const double ct = sqrt(1.0 - sin2t);
+            const double a = (n1 * c - n2 * ct) / (n1 * c + n2 * ct);
+            const double b = (n1 * ct - n2 * c) / (n1 * ct + n2 * c);
+            T = 1.0 - 0.5 * (a * a + b * b);
+        }
+    }
+    const double w_node = 0.5 * (t1 - t0) * gw * T * sn / (4.0 * 3.141592653589793);
+    const float tan_th = (float)(sn / c);
+    for (int64_t s0 = (int64_t)blockIdx.x * DIRECT_SITES_PER_CTA; s0 < A.n; s0 += (int64_t)gridDim.x * DIRECT_SITES_PER_CTA) {
+        const int64_t i = s0 + s_loc;
+        for (int t = threadIdx.x; t < DIRECT_SITES_PER_CTA * CELLS; t += blockDim.x) (&acc[0][0])[t] = 0.0f;
+        __syncthreads();
+        if (i < A.n) {
+            const float x0 = A.xyz[3 * i], y0 = A.xyz[3 * i + 1], z0 = A.xyz[3 * i + 2];
+            const float h = A.L2 - z0;
+            if (h > 0.0f && x0 >= 0.0f && x0 <= A.L0 && y0 >= 0.0f && y0 <= A.L1) {
+                const float wt = (float)(w_node * exp(-(double)A.mu * (double)h / c));
+                const float rho = h * tan_th;
+                const float inv = 1.0f / rho;
+                int ilo = (int)floorf((x0 - rho) / A.pitch), ihi = (int)floorf((x0 + rho) / A.pitch);
+                int jlo = (int)floorf((y0 - rho) / A.pitch), jhi = (int)floorf((y0 + rho) / A.pitch);
+                ilo = max(ilo, 0); jlo = max(jlo, 0); ihi = min(ihi, A.nx - 1); jhi = min(jhi, A.ny - 1);
+                for (int jj = jlo; jj <= jhi; ++jj) {
+                    const float ya = fminf(jj * A.pitch, A.L1);
+                    const float yb = jj == A.ny - 1 ? A.L1 : fminf((jj + 1) * A.pitch, A.L1);
+                    for (int ii = ilo; ii <= ihi; ++ii) {
+                        const float xa = fminf(ii * A.pitch, A.L0);
+                        const float xb = ii == A.nx - 1 ? A.L0 : fminf((ii + 1) * A.pitch, A.L0);
+                        const float arc = arc_in_box((xa - x0) * inv, (xb - x0) * inv, (ya - y0) * inv,
+                                                     (yb - y0) * inv);
+                        if (arc > 0.0f) atomicAdd(&acc[s_loc][jj * A.nx + ii], wt * arc);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < DIRECT_SITES_PER_CTA * CELLS; t += blockDim.x) {
+            const int64_t site = s0 + t / CELLS;
+            if (site < A.n) A.out[site * CELLS + t % CELLS] = (&acc[0][0])[t];
         }
         __syncthreads();
     }
@@ -391,6 +527,17 @@ int cl_surrogate_combine(const float* d_raw, int32_t members, int64_t n_sites,
                          float* d_p, float* d_tmean, float* d_tsig, float* d_spread,
                          uint8_t* d_flag, void* stream)
 {
+    return cl_surrogate_combine_direct(d_raw, members, n_sites, d_y_mean, d_y_std, d_xyz, nullptr, box, ro, pde,
+                                       spread_max, wall_min_mm, d_p, d_tmean, d_tsig, d_spread, d_flag, stream);
+}
+
+int cl_surrogate_combine_direct(const float* d_raw, int32_t members, int64_t n_sites,
+                                const float* d_y_mean, const float* d_y_std, const float* d_xyz,
+                                const float* d_direct, const cl_box* box, const cl_readout* ro, float pde,
+                                float spread_max, float wall_min_mm,
+                                float* d_p, float* d_tmean, float* d_tsig, float* d_spread,
+                                uint8_t* d_flag, void* stream)
+{
     if (!box || !ro || members < 1 || n_sites < 0) return CL_ERR_ARG;
     if ((int64_t)ro->grid.nx * ro->grid.ny != cl::sur::CELLS) return CL_ERR_ARG;
     if (n_sites == 0) return CL_OK;
@@ -399,6 +546,7 @@ int cl_surrogate_combine(const float* d_raw, int32_t members, int64_t n_sites,
     if (!(pde >= 0.0f && pde <= 1.0f)) return CL_ERR_ARG;
     cl::sur::CombineArgs a;
     a.raw = d_raw; a.K = members; a.n = n_sites; a.y_mean = d_y_mean; a.y_std = d_y_std; a.xyz = d_xyz;
+    a.direct = d_direct;
     a.L0 = box->L[0]; a.L1 = box->L[1]; a.L2 = box->L[2];
     a.front_wrapped = ro->two_sided ? 0 : 1;
     a.pde = pde; a.spread_max = spread_max; a.wall_min_mm = wall_min_mm;
@@ -406,6 +554,31 @@ int cl_surrogate_combine(const float* d_raw, int32_t members, int64_t n_sites,
     const int64_t want = (n_sites + cl::sur::SITES_PER_CTA - 1) / cl::sur::SITES_PER_CTA;
     const unsigned grid = (unsigned)(want < 148 * 64 ? want : 148 * 64);
     cl::sur::surrogate_combine<<<grid, cl::sur::CELLS * cl::sur::SITES_PER_CTA, 0, (cudaStream_t)stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
+}
+
+int cl_surrogate_direct(const float* d_xyz, int64_t n_sites, const cl_box* box, const cl_optical_params* op,
+                        const cl_readout* ro, float* d_out, void* stream)
+{
+    if (!box || !op || !ro || n_sites < 0) return CL_ERR_ARG;
+    if ((int64_t)ro->grid.nx * ro->grid.ny != cl::sur::CELLS || ro->grid.nx < 1 || !(ro->grid.pitch_mm > 0.0f))
+        return CL_ERR_ARG;
+    // the model: one full readout face at z = Lz
+    if (ro->disc || ro->two_sided) return CL_ERR_ARG;
+    if (!(op->n_crystal > 0.0f) || !(op->n_coupling > 0.0f) || !(op->abs_len_mm > 0.0f) || !(op->rayleigh_mm > 0.0f))
+        return CL_ERR_ARG;
+    if (n_sites == 0) return CL_OK;
+    if (!d_xyz || !d_out) return CL_ERR_ARG;
+    cl::sur::DirectArgs a;
+    a.xyz = d_xyz; a.n = n_sites; a.L0 = box->L[0]; a.L1 = box->L[1]; a.L2 = box->L[2];
+    a.n1 = op->n_crystal; a.n2 = op->n_coupling;
+    a.mu = (float)((std::isinf(op->abs_len_mm) ? 0.0 : 1.0 / (double)op->abs_len_mm) +
+                   (std::isinf(op->rayleigh_mm) ? 0.0 : 1.0 / (double)op->rayleigh_mm));
+    a.pitch = ro->grid.pitch_mm; a.nx = ro->grid.nx; a.ny = ro->grid.ny; a.out = d_out;
+    const int64_t want = (n_sites + cl::sur::DIRECT_SITES_PER_CTA - 1) / cl::sur::DIRECT_SITES_PER_CTA;
+    const unsigned grid = (unsigned)(want < 148 * 32 ? want : 148 * 32);
+    cl::sur::surrogate_direct<<<grid, cl::sur::DIRECT_NODES * cl::sur::DIRECT_SITES_PER_CTA, 0,
+                                (cudaStream_t)stream>>>(a);
     return cudaGetLastError() == cudaSuccess ? CL_OK : CL_ERR_CUDA;
 }
 

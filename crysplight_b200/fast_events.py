@@ -34,7 +34,7 @@ import numpy as np
 from . import _lib
 from .events import EventsResult, GammaMaterial, gamma_stage
 from .params import COUNTER_NAMES, Box, OpticalParams, Readout, TimeBinning
-from .surrogate import D_OUT, MLP, N_CELLS, LightSurrogate
+from .surrogate import D_OUT, MLP, N_CELLS, LightSurrogate, first_pass_light, first_pass_optics
 from .transport import stream_arg
 
 SPREAD_MAX = 0.02
@@ -111,6 +111,15 @@ class SurrogateEvents:
     def nets(self):
         return self.main.nets
 
+    def _check_first_pass(self, op: OpticalParams, ro: Readout):
+        """An ensemble trained on the light minus the first-pass term serves
+        only the optics that term was computed for."""
+        want = first_pass_optics(op, ro)
+        for r in [self.main] + self.experts:
+            fp = r.sur.first_pass
+            if fp is not None and not np.array_equal(np.float32(fp), np.float32(want)):
+                raise ValueError(f"the ensemble's first-pass term is for optics {fp}, the run has {want}")
+
     def close(self):
         for r in [self.main] + self.experts:
             r.close()
@@ -142,9 +151,14 @@ class SurrogateEvents:
                         torch.empty(n, dtype=torch.float32, device=self.dev),
                         torch.empty(n, dtype=torch.uint8, device=self.dev))
         P = C.c_void_p
-        rc = self.lib.cl_surrogate_combine(
+        # an ensemble trained on the light minus the first-pass term gets it back here
+        direct = None
+        if ens.sur.first_pass is not None and n:
+            direct = first_pass_light(xyz, self.box, ens.sur.first_pass, self.device, stream)
+        rc = self.lib.cl_surrogate_combine_direct(
             P(raw.data_ptr()), K, n, P(ens.y_mean.data_ptr()), P(ens.y_std.data_ptr()),
-            P(xyz.data_ptr()), C.byref(self.box), C.byref(ro), float(pde), float(spread_max),
+            P(xyz.data_ptr()), P(direct.data_ptr()) if direct is not None else None, C.byref(self.box),
+            C.byref(ro), float(pde), float(spread_max),
             float(wall_min_mm), P(out.p.data_ptr()), P(out.tmean.data_ptr()), P(out.tsig.data_ptr()),
             P(out.spread.data_ptr()), P(out.flag.data_ptr()), stream_arg(stream))
         if rc != 0:
@@ -186,6 +200,7 @@ class SurrogateEvents:
             raise ValueError("the surrogate was trained for another crystal size")
         ro = ro if isinstance(ro, Readout) else Readout(ro)
         if light is None:
+            self._check_first_pass(op, ro)
             light = self.site_light(xyz, ro=ro, pde=float(op.pde), spread_max=spread_max,
                                     wall_min_mm=wall_min_mm, stream=stream)
         return sample_sites(self.engine, box, op, ro, tb, xyz=xyz, t0=t0, photons=photons,

@@ -247,6 +247,7 @@ def scan_light(engine, box: Box, op, ro, *, points: np.ndarray, photons_per_poin
 
 
 MIN_TIME_COUNTS = 20       # below this a cell's time moments are replaced by column medians
+FIRST_PASS_FLOOR = 1e-6    # floor of a training target's probability minus its first-pass term
 SIGMA_FLOOR_NS = 1e-3
 
 
@@ -322,6 +323,39 @@ def split_holdout(n_points: int, frac: float = 0.1, seed: int = 11):
 
 
 # ---------------------------------------------------------------------------
+# First-pass light
+# ---------------------------------------------------------------------------
+def first_pass_optics(op, ro) -> tuple:
+    """The optics the first-pass term depends on: (n_crystal, n_coupling,
+    abs_len_mm, rayleigh_mm, pitch_mm, nx, ny)."""
+    ro = ro if isinstance(ro, Readout) else Readout(ro)
+    return (float(op.n_crystal), float(op.n_coupling), float(op.abs_len_mm), float(op.rayleigh_mm),
+            float(ro.grid.pitch_mm), int(ro.grid.nx), int(ro.grid.ny))
+
+
+def first_pass_light(xyz, box: Box, optics: tuple, device: int = 0, stream=None):
+    """First-pass detection probabilities (cl_surrogate_direct) of emission
+    points xyz ((n, 3) float32 CUDA tensor or array, mm): torch tensor
+    (n, 64) on the GPU.  A photon reaches the readout face without a bulk
+    interaction, is transmitted and lands in the SiPM's pixel; PDE 1."""
+    import torch
+    from .params import OpticalParams, SipmGrid
+    from .transport import stream_arg
+    x = torch.as_tensor(np.asarray(xyz, np.float32) if not isinstance(xyz, torch.Tensor) else xyz,
+                        dtype=torch.float32, device=f"cuda:{device}").contiguous()
+    n1, n2, ab, ray, pitch, nx, ny = optics
+    op = OpticalParams(n1, n2, ab, ray, 1.0, True, True, 0.0, 1.0)
+    ro = Readout(SipmGrid(pitch, int(nx), int(ny)))
+    out = torch.empty((x.shape[0], N_CELLS), dtype=torch.float32, device=x.device)
+    rc = _lib.load().cl_surrogate_direct(C.c_void_p(x.data_ptr()), int(x.shape[0]), C.byref(box),
+                                         C.byref(op), C.byref(ro), C.c_void_p(out.data_ptr()),
+                                         stream_arg(stream))
+    if rc != 0:
+        raise _lib.CudaTransportError(rc, "cl_surrogate_direct failed")
+    return out
+
+
+# ---------------------------------------------------------------------------
 # Ensemble
 # ---------------------------------------------------------------------------
 @dataclass
@@ -335,6 +369,9 @@ class LightSurrogate:
     meta: dict = field(default_factory=dict)
     z_warp: float = 0.0         # network input depth: 2 depth_warp((z - z0) / (z1 - z0)) - 1
     z_range: Optional[tuple] = None   # (z0, z1) mm of a slab ensemble; None: the whole crystal
+    # optics of the first-pass term (first_pass_optics) when the members were
+    # trained on the light response minus it; None: on the whole response
+    first_pass: Optional[tuple] = None
 
     def depth_range(self) -> tuple:
         """(z0, z1) in mm: the depths the network's input spans."""
@@ -356,7 +393,8 @@ class LightSurrogate:
     def train(cls, box: Box, xyz: np.ndarray, targets: np.ndarray, *, members: int = 5, steps: int = 20000,
               batch: int = 65536, lr: float = 1e-3, lr_final: Optional[float] = None,
               time_weight: float = 1.0, z_warp: float = 0.0, z_range=None, seed: int = 0,
-              device: int = 0, chunk: int = 250, log=None, group=None, member_trainer=None):
+              device: int = 0, chunk: int = 250, log=None, group=None, member_trainer=None,
+              first_pass: Optional[tuple] = None):
         """Train ``members`` networks on standardised targets.
 
         ``lr_final``: cosine decay of the Adam step size from ``lr`` to
@@ -371,7 +409,9 @@ class LightSurrogate:
         all_gather of the parameter vectors).  Member k's initialisation and
         minibatch stream depend on k only, so the ensemble is the same for
         any number of ranks.  ``member_trainer(k, x, y) -> (params, losses)``
-        replaces the tensor-core trainer (tests)."""
+        replaces the tensor-core trainer (tests).  ``first_pass``: the optics
+        of the first-pass term (first_pass_optics) when ``targets`` hold the
+        light response minus it (prediction adds it back)."""
         import math
         import time
         L = np.array([float(box.L[i]) for i in range(3)], np.float64)
@@ -379,7 +419,8 @@ class LightSurrogate:
         y_std = np.maximum(targets.std(0), 1e-6).astype(np.float64)
         y_std[N_CELLS:] /= math.sqrt(time_weight)
         obj = cls(L, y_mean.astype(np.float32), y_std.astype(np.float32), [], z_warp=float(z_warp),
-                  z_range=None if z_range is None else (float(z_range[0]), float(z_range[1])))
+                  z_range=None if z_range is None else (float(z_range[0]), float(z_range[1])),
+                  first_pass=None if first_pass is None else tuple(first_pass))
         xn = obj.normalise(xyz)
         yn = ((targets - y_mean) / y_std).astype(np.float32)
         if member_trainer is None:
@@ -447,6 +488,11 @@ class LightSurrogate:
         y = raw * self.y_std.astype(np.float64) + self.y_mean.astype(np.float64)
         c = self.cells
         p = np.exp(y[:, :, :c])
+        if self.first_pass is not None:
+            # the same first-pass term for every member: it moves the mean, not the spread
+            box = Box(tuple(float(v) for v in self.box_mm))
+            p = p + first_pass_light(np.asarray(xyz, np.float32).reshape(-1, 3), box, self.first_pass,
+                                     device).double().cpu().numpy()[None]
         pm = p.mean(0)
         spread = p.std(0).sum(1) / np.maximum(pm.sum(1), 1e-30)
         return {"p": pm, "t_mean": y[:, :, c:2 * c].mean(0), "t_sigma": np.exp(y[:, :, 2 * c:].mean(0)),
@@ -456,6 +502,7 @@ class LightSurrogate:
         np.savez_compressed(path, box_mm=self.box_mm, y_mean=self.y_mean, y_std=self.y_std,
                             members=np.stack(self.members), cells=self.cells, z_warp=np.float64(self.z_warp),
                             z_range=np.float64(self.depth_range() if self.z_range is not None else (np.nan, np.nan)),
+                            first_pass=np.float64(self.first_pass if self.first_pass is not None else [np.nan] * 7),
                             meta=np.array(repr({k: v for k, v in self.meta.items() if k != "loss_history"})))
 
     @classmethod
@@ -464,5 +511,9 @@ class LightSurrogate:
         zr = None
         if "z_range" in z.files and np.all(np.isfinite(z["z_range"])):
             zr = (float(z["z_range"][0]), float(z["z_range"][1]))
+        fp = None
+        if "first_pass" in z.files and not np.any(np.isnan(z["first_pass"])):
+            f = [float(v) for v in z["first_pass"]]
+            fp = (f[0], f[1], f[2], f[3], f[4], int(f[5]), int(f[6]))
         return cls(z["box_mm"], z["y_mean"], z["y_std"], list(z["members"]), int(z["cells"]),
-                   {"saved": str(z["meta"])}, float(z["z_warp"]) if "z_warp" in z.files else 0.0, zr)
+                   {"saved": str(z["meta"])}, float(z["z_warp"]) if "z_warp" in z.files else 0.0, zr, fp)

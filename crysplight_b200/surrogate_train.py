@@ -129,6 +129,11 @@ def main(argv=None):
     ap.add_argument("--z-range", type=float, nargs=2, default=None, metavar=("Z0", "Z1"),
                     help="train an expert for the depth slab z0..z1 mm (grid and network input "
                          "span the slab; the event generator uses it for sites inside)")
+    ap.add_argument("--first-pass", action="store_true",
+                    help="train on the light response minus its first-pass term (cl_surrogate_direct: "
+                         "photons that reach the readout face without an interaction), which the "
+                         "ensemble adds back exactly; the term carries the sharp pixel edges of "
+                         "sites near the readout face")
     ap.add_argument("--compare-model", default=None,
                     help="also validate this ensemble (.npz, e.g. the whole-crystal one) on the "
                          "same held-out points")
@@ -178,6 +183,16 @@ def main(argv=None):
     print(f"scan: {pts.shape[0]} points x {args.photons} photons in {scan.seconds:.1f} s "
           f"({n_ph / scan.seconds / 1e6:.0f} M photons/s)", flush=True)
     y = light_targets(scan)
+    fp = None
+    if args.first_pass:
+        from .surrogate import FIRST_PASS_FLOOR, first_pass_light, first_pass_optics
+        fp = first_pass_optics(op, ro)
+        D = first_pass_light(pts, box, fp, args.device).double().cpu().numpy()
+        p_scan_all = (scan.counts.astype(np.float64) + 0.5) / (args.photons + 1.0)
+        y[:, :64] = np.log(np.maximum(p_scan_all - D, FIRST_PASS_FLOOR)).astype(np.float32)
+        rep["first_pass"] = {"mean_sum": float(D.sum(1).mean()),
+                             "floored_cells": int((p_scan_all - D < FIRST_PASS_FLOOR).sum())}
+    rep["first_pass_optics"] = fp
     tr, ho = split_holdout(pts.shape[0], 0.1, seed=11)
     if args.model:
         sur = LightSurrogate.load(args.model)
@@ -187,7 +202,7 @@ def main(argv=None):
                                    lr_final=args.lr_final if args.lr_final >= 0 else None,
                                    time_weight=args.time_weight, z_warp=args.z_warp,
                                    z_range=args.z_range, seed=args.seed,
-                                   device=args.device, group=group,
+                                   device=args.device, group=group, first_pass=fp,
                                    log=lambda s: print(s, flush=True))
         rep["train_seconds"] = sur.meta["train_seconds"]
         rep["final_loss"] = [h[-1] for h in sur.meta["loss_history"]]
@@ -270,7 +285,7 @@ def main(argv=None):
             dist.destroy_process_group()
         return rep
     sur.meta.update({"setup": args.setup, "grid": list(args.grid), "photons_per_point": args.photons,
-                     "z_range": args.z_range})
+                     "z_range": args.z_range, "first_pass": fp})
     sur.save(args.out)
     if args.report:
         with open(args.report, "w") as f:

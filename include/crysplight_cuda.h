@@ -326,6 +326,40 @@ int cl_surrogate_combine(const float* d_raw, int32_t members, int64_t n_sites,
                          uint8_t* d_flag, void* stream);
 
 /*
+ * As cl_surrogate_combine, with d_direct [n_sites][64] (device, may be NULL):
+ * the sites' first-pass probabilities (cl_surrogate_direct) for an ensemble
+ * trained on the light response minus that term.  They are added to the
+ * members' mean before the PDE (d_p = pde * (d_direct + mean_k p_k)) and to
+ * the total the spread is relative to (d_spread = sum of the members'
+ * standard deviations / sum of (d_direct + mean_k p_k)); the members' spread
+ * itself does not include them.  No counterpart in the reference.
+ */
+int cl_surrogate_combine_direct(const float* d_raw, int32_t members, int64_t n_sites,
+                                const float* d_y_mean, const float* d_y_std, const float* d_xyz,
+                                const float* d_direct, const cl_box* box, const cl_readout* ro, float pde,
+                                float spread_max, float wall_min_mm,
+                                float* d_p, float* d_tmean, float* d_tsig, float* d_spread,
+                                uint8_t* d_flag, void* stream);
+
+/*
+ * First-pass light of n_sites emission points (no counterpart in the
+ * reference): d_out[i][c] = probability that a photon emitted isotropically
+ * at d_xyz[i] (mm) reaches the readout face z = Lz without a bulk interaction
+ * (absorption or Rayleigh scattering: survival exp(-d (1/abs_len +
+ * 1/rayleigh)) over the path d), is transmitted by the face (the Fresnel
+ * coefficients of the transport, n_crystal -> n_coupling, total internal
+ * reflection beyond the critical angle) and lands in SiPM c's pixel, at
+ * PDE 1; landing points off the face count for nothing (those photons meet a
+ * side wall first).  Computed by quadrature over the polar angle (64
+ * Gauss-Legendre nodes up to the critical angle) with the azimuthal arcs of
+ * each pixel exact.  Requires a 64-cell grid read out on the face z = Lz
+ * only (no disc, not two-sided).  Device arrays, asynchronous on `stream`;
+ * allocates nothing.
+ */
+int cl_surrogate_direct(const float* d_xyz, int64_t n_sites, const cl_box* box, const cl_optical_params* op,
+                        const cl_readout* ro, float* d_out, void* stream);
+
+/*
  * Network inputs of the surrogate for n_sites emission points (no counterpart
  * in the reference): d_out[i] = (2x/Lx - 1, 2y/Ly - 1, 2w - 1) for
  * d_xyz[i] = (x, y, z) in mm, with the depth warp

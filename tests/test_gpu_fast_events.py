@@ -240,7 +240,8 @@ def test_depth_slab_expert_serves_the_sites_inside_its_slab(engine):
     se0 = SurrogateEvents(main, engine)
     ref = light(se0)
     se0.close()
-    whole = LightSurrogate(main.box_mm, main.y_mean, main.y_std, main.members, z_range=(0.0, L[2]))
+    whole = LightSurrogate(main.box_mm, main.y_mean, main.y_std, main.members, z_range=(0.0, L[2]),
+                           first_pass=main.first_pass)
     se1 = SurrogateEvents(main, engine, experts=[whole], expert_margin_mm=1.0)
     same = light(se1)
     se1.close()
@@ -248,7 +249,8 @@ def test_depth_slab_expert_serves_the_sites_inside_its_slab(engine):
         assert np.array_equal(ref[k], same[k]), k
     # a slab over the readout half: its own input mapping, so other outputs
     z0 = 0.5 * L[2]
-    slab = LightSurrogate(main.box_mm, main.y_mean, main.y_std, main.members[:3], z_range=(z0, L[2]))
+    slab = LightSurrogate(main.box_mm, main.y_mean, main.y_std, main.members[:3], z_range=(z0, L[2]),
+                          first_pass=main.first_pass)
     se2 = SurrogateEvents(main, engine, experts=[slab], expert_margin_mm=1.0)
     mixed = light(se2)
     se2.close()

@@ -52,14 +52,37 @@ def test_csitl_teflon_ensemble_is_within_one_percent(engine):
     assert err["mean"] <= 0.01, err
 
 
-def test_bgo_esr_ensemble_meets_the_bar_where_it_serves(engine):
-    """Config 5's whole-crystal BGO+ESR ensemble: the nodes the event generator
-    takes from it (at least 1 mm from a wrapped face, member spread at most 2%;
-    the rest go to the Monte Carlo) are within 1%; the figure over all
-    held-out nodes, which include the sites the spread rule sends to the Monte
-    Carlo, is printed beside it."""
+def test_bgo_esr_ensemble_is_within_one_percent(engine):
+    """Config 5's whole-crystal BGO+ESR ensemble (trained on the light minus
+    its first-pass term, which it adds back exactly) meets the 1% bar on all
+    held-out nodes, and on the nodes the event generator takes from it (at
+    least 1 mm from a wrapped face, member spread at most 2%)."""
     err, served, n_served = _holdout(engine, "bgo_esr", "bgo_esr.npz", 128, seed=90_002)
     print(f"bgo_esr held-out error: all {err['mean']:.4f} ({err['cells']} cells), "
           f"served {served['mean']:.4f} ({n_served} nodes)")
-    assert n_served >= 64
+    assert err["cells"] > 1000
+    assert err["mean"] <= 0.01, err
+    assert n_served >= 100
     assert served["mean"] <= 0.01, served
+
+
+def test_bgo_esr_readout_face_expert_is_within_one_percent(engine):
+    """The readout-face expert (64x64x16 nodes over the last 8 mm, where a
+    site's light concentrates under one SiPM) on its own held-out nodes: within
+    1%, and its members agree to 2% on nearly all of them, so the spread rule
+    sends few sites near the readout face to the Monte Carlo."""
+    from crysplight_b200.surrogate import LightSurrogate, grid_points, scan_light, split_holdout
+    from crysplight_b200.surrogate_train import rel_error, setup
+    box, op, ro = setup("bgo_esr")
+    sur = LightSurrogate.load(os.path.join(SURROGATES, "bgo_esr_face.npz"))
+    pts = grid_points(box, (64, 64, 16), z_range=sur.z_range)
+    _, ho = split_holdout(pts.shape[0], 0.1, seed=11)
+    sub = np.sort(np.random.default_rng(5).choice(ho, size=96, replace=False))
+    truth = scan_light(engine, box, op, ro, points=pts[sub], photons_per_point=TRUTH_PHOTONS, seed=90_003,
+                       batch_points=64)
+    pred = sur.predict(pts[sub])
+    err = rel_error(pred["p"], truth.counts / float(TRUTH_PHOTONS), TRAIN_PHOTONS)
+    flagged = float(np.mean(pred["spread"] > 0.02))
+    print(f"bgo_esr_face held-out error {err['mean']:.4f} ({err['cells']} cells), spread > 2%: {flagged:.3f}")
+    assert err["mean"] <= 0.01, err
+    assert flagged <= 0.05
