@@ -363,6 +363,9 @@ __global__ void __launch_bounds__(CELLS * SITES_PER_CTA) surrogate_combine(const
 // with the arcs exact (intersections of the circle with the pixel's column
 // and row strips) and theta by composite Gauss-Legendre quadrature (8 panels
 // of 8 nodes up to the critical angle; 64 threads per site, one per node).
+// The nodes' contributions are summed as 2^-40 fixed-point integers, so the
+// result does not depend on the order the threads add them in: a site's
+// term is the same bits in any batch.
 // The rest of the light response (reflections, scattering) varies slowly
 // over the SiPM plane; a surrogate trained on it learns what the first-pass
 // term's sharp pixel edges would otherwise ask of it.
@@ -383,6 +386,7 @@ struct DirectArgs {
 };
 
 constexpr int DIRECT_NODES = 64;
+constexpr double DIRECT_FIX = 1099511627776.0;   // 2^40
 constexpr int DIRECT_SITES_PER_CTA = 4;
 constexpr float TWO_PI_ARC = 6.283185307179586f;
 
@@ -413,7 +417,7 @@ __device__ __forceinline__ float arc_in_box(float ca, float cb, float sa, float 
 
 __global__ void __launch_bounds__(DIRECT_NODES * DIRECT_SITES_PER_CTA) surrogate_direct(const DirectArgs A)
 {
-    __shared__ float acc[DIRECT_SITES_PER_CTA][CELLS];
+    __shared__ unsigned long long acc[DIRECT_SITES_PER_CTA][CELLS];
     const int q = threadIdx.x % DIRECT_NODES;
     const int s_loc = threadIdx.x / DIRECT_NODES;
     // this thread's quadrature node: panel q / 8, node q % 8 (mirror pairs)
@@ -441,7 +445,7 @@ __global__ void __launch_bounds__(DIRECT_NODES * DIRECT_SITES_PER_CTA) surrogate
     const float tan_th = (float)(sn / c);
     for (int64_t s0 = (int64_t)blockIdx.x * DIRECT_SITES_PER_CTA; s0 < A.n; s0 += (int64_t)gridDim.x * DIRECT_SITES_PER_CTA) {
         const int64_t i = s0 + s_loc;
-        for (int t = threadIdx.x; t < DIRECT_SITES_PER_CTA * CELLS; t += blockDim.x) (&acc[0][0])[t] = 0.0f;
+        for (int t = threadIdx.x; t < DIRECT_SITES_PER_CTA * CELLS; t += blockDim.x) (&acc[0][0])[t] = 0ull;
         __syncthreads();
         if (i < A.n) {
             const float x0 = A.xyz[3 * i], y0 = A.xyz[3 * i + 1], z0 = A.xyz[3 * i + 2];
@@ -461,7 +465,9 @@ __global__ void __launch_bounds__(DIRECT_NODES * DIRECT_SITES_PER_CTA) surrogate
                         const float xb = ii == A.nx - 1 ? A.L0 : fminf((ii + 1) * A.pitch, A.L0);
                         const float arc = arc_in_box((xa - x0) * inv, (xb - x0) * inv, (ya - y0) * inv,
                                                      (yb - y0) * inv);
-                        if (arc > 0.0f) atomicAdd(&acc[s_loc][jj * A.nx + ii], wt * arc);
+                        if (arc > 0.0f)
+                            atomicAdd(&acc[s_loc][jj * A.nx + ii],
+                                      __double2ull_rn((double)wt * (double)arc * DIRECT_FIX));
                     }
                 }
             }
@@ -469,7 +475,7 @@ __global__ void __launch_bounds__(DIRECT_NODES * DIRECT_SITES_PER_CTA) surrogate
         __syncthreads();
         for (int t = threadIdx.x; t < DIRECT_SITES_PER_CTA * CELLS; t += blockDim.x) {
             const int64_t site = s0 + t / CELLS;
-            if (site < A.n) A.out[site * CELLS + t % CELLS] = (&acc[0][0])[t];
+            if (site < A.n) A.out[site * CELLS + t % CELLS] = (float)((double)(&acc[0][0])[t] / DIRECT_FIX);
         }
         __syncthreads();
     }
