@@ -259,6 +259,8 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
     if ((EPI == EPI_LOSS || EPI == EPI_DSILU) && next_row0 >= 0)
         next_in = EPI == EPI_LOSS && G.trow ? (int64_t)G.trow[next_row0 + lane] : (int64_t)(next_row0 + lane);
     float sq = 0.0f;
+    // the loss targets' row: the minibatch row's training-set row
+    const int64_t trow_i = EPI == EPI_LOSS ? (G.trow ? (int64_t)G.trow[row] : (int64_t)row) : 0;
     float* xs = reinterpret_cast<float*>(stg + EpiCfg<EPI>::tiles * STAGE_TILE_BYTES);
     float x0 = 0.f, x1 = 0.f, x2 = 0.f;
     if (EPI == EPI_DSILU_L1) {
@@ -273,8 +275,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
             __syncwarp();
         }
         // the chunk's pre-activations are requested before the accumulator is
-        // read, so that their latency overlaps the tensor-memory load (the
-        // loss targets come from L2, prefetched during the previous tile)
+        // read, so that their latency overlaps the tensor-memory load
         uint4 zp4[4];
         if (EPI == EPI_DSILU) {
             const uint4* z4 = reinterpret_cast<const uint4*>(G.zprev + (int64_t)row * G.ldh + c0);
@@ -283,6 +284,14 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
         }
         float v[32];
         umma::tmem_ld32(tbase + (uint32_t)(c0 - un.n0), v);
+        // the chunk's loss targets, all requested at once (from L2: prefetched
+        // during the previous tile)
+        float4 tg[8];
+        if (EPI == EPI_LOSS) {
+            const float4* t4 = reinterpret_cast<const float4*>(G.target + trow_i * N + c0);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) tg[i] = t4[i];
+        }
         if (EPI == EPI_WGRAD) {
             // column n of the tile is row n of the transposed output: the warp's
             // 32 rows are 32 consecutive floats there (one coalesced reduction)
@@ -332,9 +341,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& G, const OutMaps& om, u
                 for (int g = 0; g < 4; ++g) {
                     float b[8];
                     cst8(cst + c0 + 8 * g, b);
-                    const int64_t tr = G.trow ? (int64_t)G.trow[row] : (int64_t)row;
-                    const float4* t4 = reinterpret_cast<const float4*>(G.target + tr * N + c0);
-                    const float4 ta = t4[2 * g], tb = t4[2 * g + 1];
+                    const float4 ta = tg[2 * g], tb = tg[2 * g + 1];
                     const float tt[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
