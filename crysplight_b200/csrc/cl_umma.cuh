@@ -160,8 +160,8 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t b
                  :: "r"(smem_u32(mbar)), "r"(bytes) : "memory");
 }
 
-// 2-D tiled TMA load, into this CTA's shared memory only, of the box at element coordinates
-// (x = inner, y = row) into shared memory; completion counted on `mbar`.
+// 2-D tiled TMA load of the box at element coordinates (x = inner, y = row)
+// into this CTA's shared memory; completion counted on `mbar`.
 __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int32_t x, int32_t y, uint64_t* mbar)
 {
     asm volatile(
