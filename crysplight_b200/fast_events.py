@@ -298,7 +298,8 @@ def sample_sites(engine, box: Box, op: OpticalParams, ro: Readout, tb: TimeBinni
         int(n_segments), ptr(maps), ptr(tmin), ptr(npe), ptr(ctr), ptr(sampled),
         stream_arg(stream))
     eng._check(rc)
-    eng.sync(stream)
+    # the site statistics are gathered while the transport runs (torch's own
+    # stream; `photons` is only read by both)
     wall = torch.from_numpy((flag_h & 2) != 0).to(dev)
     stats = {"sites": n_sites, "fallback_sites": int(fb.size), "photons_mc": n_mc,
              "photons_total": int(photons.sum().item()),
@@ -306,6 +307,7 @@ def sample_sites(engine, box: Box, op: OpticalParams, ro: Readout, tb: TimeBinni
              "flag_spread": int(np.count_nonzero(flag_h & 1)),
              "flag_wall": int(np.count_nonzero(flag_h & 2)),
              "flag_invalid": int(np.count_nonzero(flag_h & 4))}
+    eng.sync(stream)
     return (maps, tmin, npe, ctr, sampled), stats
 
 
