@@ -216,7 +216,9 @@ __device__ double emg_min(int64_t k, double mu, double sigma, double tau, Uni& U
     return mu + sigma * z;
 }
 
-__global__ void __launch_bounds__(128) surrogate_sample(const SurSampleArgs A)
+// Eight CTAs of 128 threads per SM (64 registers; the Float64 special
+// functions' latency needs the warps more than the spilled registers cost).
+__global__ void __launch_bounds__(128, 8) surrogate_sample(const SurSampleArgs A)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     unsigned bad = 0;
