@@ -41,7 +41,9 @@
 namespace cl {
 namespace sur {
 
-constexpr uint32_t STREAM_TAG = 0x53555247u;   // "SURG"
+constexpr uint32_t STREAM_TAG = 0x53555247u;   // "SURG": a site's binomial chain
+constexpr uint32_t TIME_TAG = 0x53555254u;     // "SURT": a (site, SiPM) first-hit time
+constexpr int CELLS = 64;                      // SiPMs of the readout grid
 constexpr unsigned SAMPLER_BUDGET_BIT = 4u;
 
 // Float64 uniforms in (0, 1) from one Philox stream.
@@ -188,10 +190,9 @@ __device__ double emg_cdf(double z, double ls, double lam, double* dens)
 }
 
 // Minimum of k >= 1 independent EMG(mu, sigma, tau) arrival times, by
-// inverting P(min <= t) = 1 - (1 - F(t))^k at one uniform.
-__device__ double emg_min(int64_t k, double mu, double sigma, double tau, Uni& U, unsigned& bad)
+// inverting P(min <= t) = 1 - (1 - F(t))^k at the uniform u in (0, 1).
+__device__ double emg_min_u(int64_t k, double mu, double sigma, double tau, double u, unsigned& bad)
 {
-    const double u = U.next();
     const double lu = log(u) / (double)k;       // log of the survival level, < 0
     const double y = -expm1(lu);                // target F(t) in (0, 1)
     if (!(tau > 0.0)) return mu + sigma * normcdfinv(y);
@@ -216,40 +217,99 @@ __device__ double emg_min(int64_t k, double mu, double sigma, double tau, Uni& U
     return mu + sigma * z;
 }
 
-// Eight CTAs of 128 threads per SM (64 registers; the Float64 special
-// functions' latency needs the warps more than the spilled registers cost).
-__global__ void __launch_bounds__(128, 8) surrogate_sample(const SurSampleArgs A)
+__device__ double emg_min(int64_t k, double mu, double sigma, double tau, Uni& U, unsigned& bad)
 {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    return emg_min_u(k, mu, sigma, tau, U.next(), bad);
+}
+
+// The uniform of the first-hit time of SiPM c at site i: word 0 of its own
+// Philox block (counter (site lo, site hi, c, "SURT")), disjoint from the
+// site's binomial stream and from the transport's photon streams.
+__device__ __forceinline__ double time_uniform(int64_t i, int c, uint32_t k0, uint32_t k1)
+{
+    const uint4 o = philox4x32_10(make_uint4((uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)c, TIME_TAG),
+                                  k0, k1);
+    return ((double)o.x + 0.5) * 0x1p-32;
+}
+
+// Warp-cooperative: each lane runs the binomial chain of one site (the
+// chain is sequential over the SiPMs), recording the hit counts in shared
+// memory; then the warp's lanes share out the first-hit times of all
+// (site, SiPM) pairs that were hit, which cost far more than the chain (a
+// safeguarded Newton inversion in Float64 each) and which thread-per-site
+// code would leave to the lanes of the sites with the most hit SiPMs.  Each
+// pair's time comes from its own uniform (time_uniform), so the result does
+// not depend on which lane draws it.  Eight CTAs of 128 threads per SM
+// (64 registers; the Float64 special functions' latency needs the warps more
+// than the spilled registers cost).
+constexpr int SAMPLE_WARPS = 4;
+__global__ void __launch_bounds__(32 * SAMPLE_WARPS, 8) surrogate_sample(const SurSampleArgs A)
+{
+    __shared__ uint16_t s_k[SAMPLE_WARPS][CELLS][32];   // hit counts of the warp's sites, by SiPM
+    __shared__ uint32_t s_mask[SAMPLE_WARPS][CELLS];    // lanes whose site hit the SiPM
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cells = A.cells;                          // <= CELLS (launcher)
+    const int64_t nwarps = (int64_t)gridDim.x * SAMPLE_WARPS;
     unsigned bad = 0;
     unsigned long long ph = 0, det = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
-        if (A.flag && A.flag[i]) continue;
-        int64_t left = A.photons[i];
-        if (left <= 0) continue;
+    for (int64_t i0 = ((int64_t)blockIdx.x * SAMPLE_WARPS + wib) * 32; i0 < A.n; i0 += nwarps * 32) {
+        // ---- the binomial chain of this lane's site ----
+        const int64_t i = i0 + lane;
+        int64_t left = 0, base = 0;
+        if (i < A.n && !(A.flag && A.flag[i])) {
+            left = A.photons[i];
+            if (left > 0) {
+                const int32_t sg = A.seg[i];
+                if (sg < 0 || (int64_t)sg >= A.n_seg) { bad |= 8u; left = 0; }
+                else { base = (int64_t)sg * cells; ph += (unsigned long long)left; }
+            } else {
+                left = 0;
+            }
+        }
         Uni U;
         U.init((uint64_t)i, A.k0, A.k1);
-        const float* p = A.p + i * A.cells;
-        const float* tm = A.tmean + i * A.cells;
-        const float* ts = A.tsig + i * A.cells;
-        const double t0 = (double)A.t0[i];
-        const int32_t sg = A.seg[i];
-        if (sg < 0 || (int64_t)sg >= A.n_seg) { bad |= 8u; continue; }
-        ph += (unsigned long long)left;
-        const int64_t base = (int64_t)sg * A.cells;
+        const float* p = A.p + i * cells;
         double mass = 1.0;                          // probability not yet assigned
-        for (int c = 0; c < A.cells && left > 0; ++c) {
-            const double pc = (double)p[c];
-            const double pcond = mass > 0.0 ? fmin(fmax(pc / mass, 0.0), 1.0) : 1.0;
-            mass -= pc;
-            const int64_t k = binomial(left, pcond, U, bad);
-            if (k <= 0) continue;
-            left -= k;
-            det += (unsigned long long)k;
-            atomicAdd(A.maps + base + c, (uint32_t)k);
-            const double t = emg_min(k, (double)tm[c], (double)ts[c], (double)A.tau, U, bad);
-            atomicMin(A.keys + base + c, float_key((float)(t0 + t)));
+        for (int c = 0; c < cells; ++c) {
+            int64_t k = 0;
+            if (left > 0) {
+                const double pc = (double)p[c];
+                const double pcond = mass > 0.0 ? fmin(fmax(pc / mass, 0.0), 1.0) : 1.0;
+                mass -= pc;
+                k = binomial(left, pcond, U, bad);
+                if (k > 0) {
+                    left -= k;
+                    det += (unsigned long long)k;
+                    atomicAdd(A.maps + base + c, (uint32_t)k);
+                    if (k > 65535) {
+                        // beyond the shared counts' range: this lane draws its time now
+                        const double t = emg_min_u(k, (double)A.tmean[i * cells + c], (double)A.tsig[i * cells + c],
+                                                   (double)A.tau, time_uniform(i, c, A.k0, A.k1), bad);
+                        atomicMin(A.keys + base + c, float_key((float)((double)A.t0[i] + t)));
+                        k = 0;
+                    }
+                }
+            }
+            s_k[wib][c][lane] = (uint16_t)k;
+            const unsigned m = __ballot_sync(0xffffffffu, k > 0);
+            if (lane == 0) s_mask[wib][c] = m;
         }
+        __syncwarp();
+        // ---- the first-hit times of every (site, SiPM) pair hit, shared out ----
+        int total = 0;
+        for (int c = 0; c < cells; ++c) total += __popc(s_mask[wib][c]);
+        int c = 0, before = 0;                      // items of SiPMs < c
+        for (int item = lane; item < total; item += 32) {
+            while (item >= before + __popc(s_mask[wib][c])) { before += __popc(s_mask[wib][c]); ++c; }
+            const unsigned m = s_mask[wib][c];
+            const int sl = (int)__fns(m, 0u, item - before + 1);     // the site's lane
+            const int64_t is = i0 + sl;
+            const int64_t kk = s_k[wib][c][sl];
+            const double t = emg_min_u(kk, (double)A.tmean[is * cells + c], (double)A.tsig[is * cells + c],
+                                       (double)A.tau, time_uniform(is, c, A.k0, A.k1), bad);
+            atomicMin(A.keys + (int64_t)A.seg[is] * cells + c, float_key((float)((double)A.t0[is] + t)));
+        }
+        __syncwarp();
     }
     if (A.stats) {
         // one pair of atomics per warp
@@ -284,7 +344,6 @@ struct CombineArgs {
     uint8_t* flag;
 };
 
-constexpr int CELLS = 64;
 constexpr int SITES_PER_CTA = 4;
 
 __global__ void __launch_bounds__(CELLS * SITES_PER_CTA) surrogate_combine(const CombineArgs A)
@@ -518,9 +577,10 @@ __global__ void debug_sampler(int fn, double p0, double p1, double p2, double p3
 cudaError_t launch_surrogate_sample(const SurSampleArgs& a, int num_sms, cudaStream_t st)
 {
     if (a.n <= 0) return cudaSuccess;
-    const int64_t want = (a.n + 127) / 128;
+    if (a.cells < 1 || a.cells > sur::CELLS) return cudaErrorInvalidValue;
+    const int64_t want = (a.n + 32 * sur::SAMPLE_WARPS - 1) / (32 * sur::SAMPLE_WARPS);
     const int64_t cap = (int64_t)num_sms * 16;
-    sur::surrogate_sample<<<(unsigned)(want < cap ? want : cap), 128, 0, st>>>(a);
+    sur::surrogate_sample<<<(unsigned)(want < cap ? want : cap), 32 * sur::SAMPLE_WARPS, 0, st>>>(a);
     return cudaGetLastError();
 }
 
