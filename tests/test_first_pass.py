@@ -65,3 +65,19 @@ def test_surrogate_keeps_its_first_pass_optics(tmp_path):
         s.save(p)
         t = LightSurrogate.load(p)
         assert t.first_pass == f and t.z_range == (14.4, 22.4)
+
+
+def test_event_generator_refuses_other_optics():
+    from types import SimpleNamespace
+    from crysplight_b200.fast_events import SurrogateEvents
+    from crysplight_b200.surrogate import first_pass_optics
+    from crysplight_b200.params import OpticalParams
+    se = SurrogateEvents.__new__(SurrogateEvents)       # the check alone, no networks on a GPU
+    se.main = SimpleNamespace(sur=SimpleNamespace(first_pass=first_pass_optics(OP, RO)))
+    se.experts = []
+    se._check_first_pass(OP, RO)                          # the optics it was trained for
+    other = OpticalParams(2.15, 1.50, 20000.0, 2222.0, 0.985, True, True, 0.0227, 0.4)
+    with pytest.raises(ValueError, match="first-pass"):
+        se._check_first_pass(other, RO)
+    se.main = SimpleNamespace(sur=SimpleNamespace(first_pass=None))   # whole-response ensembles: any optics
+    se._check_first_pass(other, RO)
