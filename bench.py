@@ -259,6 +259,8 @@ def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wal
     mm = m_maps.cpu().numpy().view(np.uint32).reshape(n_seg, 64)
     pk_s, pk_m = photopeak(s_npe, g.edep), photopeak(m_npe.cpu().numpy(), g.edep)
     cmp = compare_maps(s_maps.T.reshape(8, 8, n_seg), mm.T.reshape(8, 8, n_seg))
+    tcmp = compare_first_times(tmin.cpu().numpy().reshape(n_seg, 64), s_maps,
+                               m_tmin.cpu().numpy().reshape(n_seg, 64), mm)
     # end to end: the public call (host gamma stage, copies in, maps out)
     se.run_events(E["box"], E["op"], E["ro"], E["tb"], E["mat"], E["yield_"], n_events=n_seg,
                   seed=E["seed"], tau_ns=E["tau"], wall_min_mm=wall_min_mm)
@@ -284,8 +286,29 @@ def run_surrogate_events_bench(eng, E, steps: int, warmup: int, dev, stream, wal
                 mc_s=mc_s, mc_photon_steps=mc_steps, photons=int(off[-1]), deposits=nd,
                 members=len(sur.members), experts=len(experts), launches=launches,
                 stats=stats, photopeak_surrogate=pk_s, photopeak_mc=pk_m,
-                photopeak_shift=(pk_s["mean"] - pk_m["mean"]) / pk_m["mean"], maps=cmp,
+                photopeak_shift=(pk_s["mean"] - pk_m["mean"]) / pk_m["mean"], maps=cmp, first_times=tcmp,
                 h2d=int(12 * nd + 4 * nd + 8 * nd + 4 * nd), d2h=int(2 * 4 * 64 * n_seg + 4 * n_seg + 72 + 16 + nd))
+
+
+def compare_first_times(t_a, maps_a, t_b, maps_b) -> dict:
+    """Per-SiPM first-hit times of two event samples over the same events: for
+    each SiPM, the mean over the events where both have hits; the mean and the
+    largest absolute difference of those means over the SiPMs (ns), the
+    largest in units of its standard error, and the overall mean time."""
+    both = (maps_a > 0) & (maps_b > 0) & np.isfinite(t_a) & np.isfinite(t_b)
+    diffs, zs = [], []
+    for c in range(t_a.shape[1]):
+        m = both[:, c]
+        if m.sum() < 20:
+            continue
+        d = t_a[m, c].astype(np.float64) - t_b[m, c]
+        diffs.append(d.mean())
+        zs.append(abs(d.mean()) / max(d.std(ddof=1) / np.sqrt(m.sum()), 1e-12))
+    diffs = np.abs(np.array(diffs))
+    return {"sipms": int(diffs.size), "mean_abs_diff_ns": float(diffs.mean()) if diffs.size else None,
+            "max_abs_diff_ns": float(diffs.max()) if diffs.size else None,
+            "max_z": float(max(zs)) if zs else None,
+            "mean_first_time_ns": float(np.mean(t_b[both])) if both.any() else None}
 
 
 def events_cpu_baseline(E, target_s: float) -> dict:
@@ -712,6 +735,7 @@ def run_cuda_arm(args, W, rank, world, local_rank):
             "speedup_vs_plain_mc": r["value"] / r["mc_value"],
             "ceiling_speedup": r["ceiling_speedup"],
             "photopeak_shift": r["photopeak_shift"], "maps_vs_mc": r["maps"],
+            "first_times_vs_mc": r["first_times"],
             "fallback_sites": r["stats"]["fallback_sites"], "sites": r["stats"]["sites"],
             "readout_face_expert": bool(r["experts"])}
     print(json.dumps(line), flush=True)
@@ -923,7 +947,7 @@ def run_surrogate_events_arm(args, rank, world, local_rank):
                 "speedup_vs_plain_mc": r["value"] / r["mc_value"],
                 "sites": r["stats"], "photopeak_surrogate": r["photopeak_surrogate"],
                 "photopeak_mc": r["photopeak_mc"], "photopeak_shift": r["photopeak_shift"],
-                "maps_vs_mc": r["maps"], "clocks": clk}
+                "maps_vs_mc": r["maps"], "first_times_vs_mc": r["first_times"], "clocks": clk}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = events_cpu_baseline(E, args.cpu_seconds)
         print(json.dumps(line), flush=True)
