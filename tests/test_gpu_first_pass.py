@@ -106,3 +106,18 @@ def test_combine_direct_adds_the_term_to_mean_and_total():
     assert np.allclose(o["sp"], spread, rtol=1e-4)
     assert np.array_equal(o["fl"] & 1, (spread > 0.02).astype(np.uint8))
     assert (o["fl"][:12] & 1).all()      # the disagreeing members
+
+
+def test_direct_has_the_same_bits_in_any_batch():
+    """A site's first-pass term does not depend on the other sites of the
+    call (its contributions are summed as fixed-point integers), so an expert
+    evaluated on a subset of the sites gives the main ensemble's bits."""
+    rng = np.random.default_rng(9)
+    L = (48.0, 48.0, 22.4)
+    xyz = (rng.uniform(0, 1, (4000, 3)) * [48.0, 48.0, 8.0] + [0.0, 0.0, 14.4]).astype(np.float32)
+    op = OpticalParams(2.15, 1.45, 20000.0, 2222.0, 0.985, True, True, 0.0227, 1.0)
+    full = _direct_gpu(xyz, Box(L), op, Readout(GRID))
+    idx = np.sort(rng.choice(4000, 1234, replace=False))
+    sub = _direct_gpu(xyz[idx], Box(L), op, Readout(GRID))
+    again = _direct_gpu(xyz, Box(L), op, Readout(GRID))
+    assert np.array_equal(full[idx], sub) and np.array_equal(full, again)
